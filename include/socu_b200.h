@@ -1,0 +1,115 @@
+/*
+ * socu_b200 — C ABI of the B200 (sm_100a) nested-dissection block-tridiagonal
+ * SPD Cholesky.
+ *
+ * Plain pointers and sizes only.  Every array pointer is a CUDA device pointer
+ * to a contiguous row-major buffer; `stream` is a cudaStream_t (NULL = legacy
+ * default stream).  All entry points return an int status (SOCU_OK == 0,
+ * negative on error) and never allocate on the hot path.
+ *
+ * Layouts (identical to socu; socu/block_tridiag_solver.py:739-774):
+ *   L     (batch, horizon, n, n)        diagonal blocks; lower triangle read
+ *   E     (batch, storage_len, n, n)    off-diagonal blocks, storage_len =
+ *                                       socu_off_diag_storage_len(horizon);
+ *                                       E[k] = Psi_{k+1,k} for k < horizon-1,
+ *                                       slots >= horizon-1 MUST be zero
+ *   x     (batch, horizon, n, n_rhs)    right-hand side in, result out
+ *   mask  (batch,) uint8 or NULL        0 = leave that batch entry untouched
+ * The factor is written in place into L and E with the reference's exact
+ * block layout, so factors are interchangeable with socu's.
+ */
+#ifndef SOCU_B200_H
+#define SOCU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOCU_OK 0
+#define SOCU_ERR_INVALID_ARGUMENT (-1)
+#define SOCU_ERR_CUDA (-2)
+#define SOCU_ERR_UNSUPPORTED (-3)
+#define SOCU_ERR_TIMEOUT (-4)
+
+typedef enum socu_dtype { SOCU_FLOAT32 = 0, SOCU_FLOAT64 = 1 } socu_dtype;
+
+typedef enum socu_op {
+  SOCU_OP_FACTOR = 0,
+  SOCU_OP_FACTOR_AND_SOLVE = 1,
+  SOCU_OP_FORWARD_SUBSTITUTION = 2,
+  SOCU_OP_BACKWARD_SUBSTITUTION = 3,
+  SOCU_OP_SOLVE = 4
+} socu_op;
+
+/* Library version string. */
+const char* socu_version(void);
+
+/* Human-readable text for a status code. */
+const char* socu_status_string(int status);
+
+/* The last CUDA error seen by this library in the calling thread (0 if none). */
+int socu_last_cuda_error(void);
+
+/* floor(log2(horizon)) + 1, or -1 for horizon <= 0.
+ * Replaces calculate_recursive_iterations, socu/block_tridiag_solver.py:12-15. */
+int64_t socu_recursive_iterations(int64_t horizon);
+
+/* Number of n x n blocks E must hold, or -1 for horizon <= 0.
+ * Replaces calculate_off_diag_storage_len, socu/block_tridiag_solver.py:18-23. */
+int64_t socu_off_diag_storage_len(int64_t horizon);
+
+/* Largest block size n supported for a dtype (shared-memory bound). */
+int64_t socu_max_block_size(socu_dtype dtype, int64_t n_rhs);
+
+/* One-shot operations, enqueued on `stream`.
+ * Replace the callbacks returned by create_cholesky_factor_launch
+ * (socu/block_tridiag_solver.py:739-923), create_cholesky_factor_and_solve_launch
+ * (:926-1233), create_cholesky_forward_substitution_launch (:1236-1374),
+ * create_cholesky_backward_substitution_launch (:1377-1517) and
+ * create_cholesky_solve_launch (:1520-1727). */
+int socu_cholesky_factor(socu_dtype dtype, void* L, void* E, const uint8_t* mask,
+                         int64_t batch, int64_t horizon, int64_t n, void* stream);
+
+int socu_cholesky_factor_and_solve(socu_dtype dtype, void* L, void* E, void* x,
+                                   const uint8_t* mask, int64_t batch, int64_t horizon,
+                                   int64_t n, int64_t n_rhs, void* stream);
+
+int socu_cholesky_forward_substitution(socu_dtype dtype, const void* L, const void* E, void* x,
+                                       const uint8_t* mask, int64_t batch, int64_t horizon,
+                                       int64_t n, int64_t n_rhs, void* stream);
+
+int socu_cholesky_backward_substitution(socu_dtype dtype, const void* L, const void* E, void* x,
+                                        const uint8_t* mask, int64_t batch, int64_t horizon,
+                                        int64_t n, int64_t n_rhs, void* stream);
+
+int socu_cholesky_solve(socu_dtype dtype, const void* L, const void* E, void* x,
+                        const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n,
+                        int64_t n_rhs, void* stream);
+
+/* Recorded launches bound to fixed buffers, optionally captured once into a
+ * CUDA graph at creation (the recorded launches + create_cuda_graph_callback
+ * of socu/block_tridiag_solver.py:784-790 and socu/utils.py:39-65).  The mask
+ * pointer is bound, its contents may change between runs (also under a
+ * graph).  `x` is ignored for SOCU_OP_FACTOR.  A launch object must not be
+ * run from two host threads at once. */
+typedef struct socu_launch_s* socu_launch_t;
+
+int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E,
+                       void* x, const uint8_t* mask, int64_t batch, int64_t horizon,
+                       int64_t n, int64_t n_rhs, int use_cuda_graph, void* stream);
+
+int socu_launch_run(socu_launch_t launch, void* stream);
+
+/* Number of kernels one run enqueues (0 for a NULL launch). */
+int64_t socu_launch_kernel_count(socu_launch_t launch);
+
+int socu_launch_destroy(socu_launch_t launch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOCU_B200_H */

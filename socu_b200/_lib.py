@@ -1,0 +1,95 @@
+"""ctypes binding of the native library ``socu_b200/lib/libsocu_b200.so``.
+
+The library is the only compute path: there is no CPU or PyTorch fallback.
+If it is missing, every solver entry point raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import threading
+
+LIB_DIR = pathlib.Path(__file__).resolve().parent / "lib"
+LIB_PATH = LIB_DIR / "libsocu_b200.so"
+
+SOCU_OK = 0
+STATUS_TEXT = {
+    0: "ok",
+    -1: "invalid argument",
+    -2: "CUDA error",
+    -3: "unsupported problem size",
+    -4: "device wait timed out",
+}
+
+FLOAT32 = 0
+FLOAT64 = 1
+
+OP_FACTOR = 0
+OP_FACTOR_AND_SOLVE = 1
+OP_FORWARD = 2
+OP_BACKWARD = 3
+OP_SOLVE = 4
+
+_lock = threading.Lock()
+_lib = None
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_u8p = ctypes.c_void_p
+
+_SIGNATURES = {
+    "socu_version": (ctypes.c_char_p, []),
+    "socu_status_string": (ctypes.c_char_p, [_int]),
+    "socu_last_cuda_error": (_int, []),
+    "socu_recursive_iterations": (_i64, [_i64]),
+    "socu_off_diag_storage_len": (_i64, [_i64]),
+    "socu_max_block_size": (_i64, [_int, _i64]),
+    "socu_cholesky_factor": (_int, [_int, _vp, _vp, _u8p, _i64, _i64, _i64, _vp]),
+    "socu_cholesky_factor_and_solve": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
+    "socu_cholesky_forward_substitution": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
+    "socu_cholesky_backward_substitution": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
+    "socu_cholesky_solve": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
+    "socu_launch_create": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p,
+                                  _i64, _i64, _i64, _i64, _int, _vp]),
+    "socu_launch_run": (_int, [_vp, _vp]),
+    "socu_launch_kernel_count": (_i64, [_vp]),
+    "socu_launch_destroy": (_int, [_vp]),
+}
+
+
+def exported_symbols():
+    """Names the C ABI declares (include/socu_b200.h)."""
+    return list(_SIGNATURES)
+
+
+def load():
+    """Load (once) and return the native library; raise RuntimeError if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = os.environ.get("SOCU_B200_LIB", str(LIB_PATH))
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"socu_b200 native library not found at {path}; build it with "
+                "`python -m socu_b200.build` (nvcc, sm_100a)")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(status: int, what: str):
+    if status != SOCU_OK:
+        lib = load()
+        detail = STATUS_TEXT.get(status, "unknown status")
+        cuda = lib.socu_last_cuda_error()
+        extra = f" (cudaError {cuda})" if status == -2 else ""
+        raise RuntimeError(f"{what} failed: {detail}{extra}")

@@ -1,0 +1,253 @@
+"""Drop-in replacement of ``socu.block_tridiag_solver`` on B200 (sm_100a).
+
+Same function names, keyword arguments, array layouts, mask semantics and
+error behaviour as the reference (socu/block_tridiag_solver.py:12-60 and
+:739-1727).  Arrays are PyTorch CUDA tensors (or any object exposing
+``__cuda_array_interface__``, e.g. a Warp array, which is wrapped without a
+copy).  Each ``create_*_launch`` validates its arguments, binds the buffers
+and returns a zero-argument callable that enqueues the hand-written CUDA
+kernels of ``libsocu_b200.so`` on the chosen stream; ``use_cuda_graph=True``
+captures them once, natively, into a CUDA graph.
+
+There is no CPU path: CPU tensors are rejected with ``ValueError`` after the
+shape checks (the reference would run them through Warp's CPU backend).
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import torch
+
+from . import _lib
+
+__all__ = [
+    "calculate_recursive_iterations",
+    "calculate_off_diag_storage_len",
+    "optimal_problem_settings",
+    "create_cholesky_factor_launch",
+    "create_cholesky_factor_and_solve_launch",
+    "create_cholesky_forward_substitution_launch",
+    "create_cholesky_backward_substitution_launch",
+    "create_cholesky_solve_launch",
+]
+
+
+def calculate_recursive_iterations(horizon: int) -> int:
+    """floor(log2(horizon)) + 1 (socu/block_tridiag_solver.py:12-15)."""
+    assert horizon > 0
+    return int(horizon).bit_length()
+
+
+def calculate_off_diag_storage_len(horizon: int) -> int:
+    """Number of off-diagonal blocks E must hold (socu/block_tridiag_solver.py:18-23)."""
+    iterations = calculate_recursive_iterations(horizon)
+    return sum(horizon // (2 ** i) - 1 for i in range(iterations))
+
+
+def _dtype_name(dtype) -> str:
+    """Accepts torch dtypes, numpy dtypes, strings and Warp scalar types."""
+    if dtype is None:
+        return "float64"
+    if isinstance(dtype, torch.dtype):
+        return {torch.float64: "float64", torch.float32: "float32"}.get(dtype, str(dtype))
+    name = getattr(dtype, "__name__", None) or getattr(dtype, "name", None) or str(dtype)
+    name = str(name).rsplit(".", 1)[-1]
+    return {"double": "float64", "float": "float32"}.get(name, name)
+
+
+def _torch_dtype(dtype):
+    name = _dtype_name(dtype)
+    if name == "float64":
+        return torch.float64
+    if name == "float32":
+        return torch.float32
+    raise ValueError("dtype must be wp.float64 or wp.float32")
+
+
+def optimal_problem_settings(n: int, dtype):
+    """Same keys and values as the reference (socu/block_tridiag_solver.py:26-60).
+
+    ``block_dim`` / ``block_size`` do not steer the B200 kernels (their tiling
+    is fixed per n); ``pad_multiple`` drives the JAX frontend's padding.
+    """
+    name = _dtype_name(dtype)
+    if name == "float64":
+        factor_fuse_threshold, solve_fuse_threshold = 16, 32
+        pad_multiple_fuse, pad_multiple_blocked = 2, 8
+    elif name == "float32":
+        factor_fuse_threshold, solve_fuse_threshold = 32, 32
+        pad_multiple_fuse, pad_multiple_blocked = 4, 16
+    else:
+        raise ValueError("dtype must be wp.float64 or wp.float32")
+    settings = {
+        "block_dim": {"factor": 64, "solve": 64},
+        "block_size": {
+            "factor": 32 if n % 32 == 0 else 16,
+            "solve": 32 if n % 32 == 0 else 16,
+        },
+        "pad_multiple": {
+            "factor": pad_multiple_fuse if n < factor_fuse_threshold else pad_multiple_blocked,
+            "solve": pad_multiple_fuse if n < solve_fuse_threshold else pad_multiple_blocked,
+        },
+    }
+    if n < factor_fuse_threshold:
+        settings["block_size"]["factor"] = factor_fuse_threshold
+    if n < solve_fuse_threshold:
+        settings["block_size"]["solve"] = solve_fuse_threshold
+    return settings
+
+
+# ---------------------------------------------------------------------------
+# argument handling
+# ---------------------------------------------------------------------------
+
+def _as_tensor(a):
+    if isinstance(a, torch.Tensor):
+        return a
+    if hasattr(a, "__cuda_array_interface__"):
+        return torch.as_tensor(a, device="cuda")
+    raise TypeError(f"expected a torch.Tensor or a __cuda_array_interface__ array, got {type(a)!r}")
+
+
+def _is_bool(mask) -> bool:
+    if isinstance(mask, torch.Tensor):
+        return mask.dtype == torch.bool
+    dt = getattr(mask, "dtype", None)
+    return _dtype_name(dt) in ("bool", "bool_")
+
+
+def _stream_handle(stream, device):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    if hasattr(stream, "cuda_stream"):
+        return int(stream.cuda_stream)
+    raise TypeError(f"unsupported stream object {type(stream)!r}")
+
+
+def _validate(L, E, x, mask, with_x: bool):
+    """Shape checks in the reference's order and with its messages
+    (socu/block_tridiag_solver.py:749-774 and :937-966)."""
+    if with_x:
+        assert E.ndim == L.ndim and x.ndim == L.ndim, "L, E, and x must have the same number of dimensions"
+    else:
+        assert E.ndim == L.ndim, "L and E must have the same number of dimensions"
+    if L.ndim == 4:
+        batch_dim = L.shape[0]
+    elif L.ndim == 3:
+        batch_dim = 1
+        L = L.reshape((1, *L.shape))
+        E = E.reshape((1, *E.shape))
+        if with_x:
+            x = x.reshape((1, *x.shape))
+    else:
+        raise ValueError("L must have 4 or 3 dimensions")
+    if with_x:
+        assert E.shape[0] == batch_dim and x.shape[0] == batch_dim, "L, E, and x must have same batch dimension"
+    else:
+        assert E.shape[0] == batch_dim, "L and E must have same batch dimension"
+    horizon = L.shape[1]
+    n = L.shape[2]
+    assert L.shape[3] == n, "The last two dimensions of L must be the same"
+    assert E.shape[2] == n and E.shape[3] == n, "L and E must have same block size"
+    n_E = calculate_off_diag_storage_len(horizon)
+    assert E.shape[1] == n_E, "E has incorrect size, use calculate_off_diag_storage_len to calculate the correct number of blocks"
+    n_rhs = 0
+    if with_x:
+        n_rhs = x.shape[3]
+        assert x.shape[1] == horizon and x.shape[2] == n, "x has incorrect dimensions"
+    if mask is not None:
+        assert mask.ndim == 1 and mask.shape[0] == batch_dim, "mask must have shape (batch_dim,)"
+        assert _is_bool(mask), "mask must be a wp.bool array"
+    return L, E, x, batch_dim, horizon, n, n_rhs
+
+
+def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x):
+    L, E = _as_tensor(L), _as_tensor(E)
+    x = _as_tensor(x) if with_x else None
+    mask = _as_tensor(mask) if mask is not None else None
+    L, E, x, batch, horizon, n, n_rhs = _validate(L, E, x, mask, with_x)
+    tdt = _torch_dtype(dtype)
+    optimal_problem_settings(n, dtype)  # dtype check, as the reference does
+    arrays = [("L", L), ("E", E)] + ([("x", x)] if with_x else [])
+    for name, a in arrays:
+        if a.device.type != "cuda":
+            if use_cuda_graph:
+                raise ValueError("use_cuda_graph=True requires a CUDA device")
+            raise ValueError(f"socu_b200 runs on CUDA devices only; {name} is on {a.device}")
+        assert a.dtype == tdt, f"{name} must have dtype {tdt}, got {a.dtype}"
+        assert a.is_contiguous(), f"{name} must be contiguous"
+    if device is not None and torch.device(device).type != "cuda":
+        raise ValueError("socu_b200 runs on CUDA devices only")
+    dev = L.device
+    for name, a in arrays[1:]:
+        assert a.device == dev, f"{name} must be on {dev}"
+    if mask is not None:
+        assert mask.device == dev and mask.is_contiguous(), "mask must be a contiguous array on the solver's device"
+
+    lib = _lib.load()
+    dt = _lib.FLOAT64 if tdt == torch.float64 else _lib.FLOAT32
+    sh = _stream_handle(stream, dev)
+    handle = ctypes.c_void_p()
+    with torch.cuda.device(dev):
+        cap_stream = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
+        status = lib.socu_launch_create(
+            ctypes.byref(handle), op, dt,
+            L.data_ptr(), E.data_ptr() if E.numel() else None,
+            x.data_ptr() if with_x else None,
+            mask.data_ptr() if mask is not None else None,
+            batch, horizon, n, n_rhs, int(bool(use_cuda_graph)), cap_stream)
+    _lib.check(status, "socu_launch_create")
+    keep = (L, E, x, mask)
+    h = handle.value
+
+    def callback():
+        s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.socu_launch_run(h, s), "socu_launch_run")
+
+    callback._socu_arrays = keep
+    callback.kernel_count = int(lib.socu_launch_kernel_count(h))
+    callback.uses_cuda_graph = bool(use_cuda_graph)
+    weakref.finalize(callback, lib.socu_launch_destroy, h)
+    return callback
+
+
+# ---------------------------------------------------------------------------
+# public factories (socu/block_tridiag_solver.py:739-1727)
+# ---------------------------------------------------------------------------
+
+def create_cholesky_factor_launch(L, E, mask=None, block_dim=None, block_size=None,
+                                  dtype=torch.float64, device=None, stream=None,
+                                  use_cuda_graph=False):
+    """In-place ND Cholesky factor of (L, E); returns a zero-argument callable."""
+    return _create(_lib.OP_FACTOR, L, E, None, mask, dtype, device, stream, use_cuda_graph, False)
+
+
+def create_cholesky_factor_and_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
+                                            dtype=torch.float64, device=None, stream=None,
+                                            use_cuda_graph=False):
+    """Factor fused with the forward sweep, then the backward sweep; x: b in, solution out."""
+    return _create(_lib.OP_FACTOR_AND_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+
+
+def create_cholesky_forward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
+                                                dtype=torch.float64, device=None, stream=None,
+                                                use_cuda_graph=False):
+    """Forward sweep on a stored factor; x: b in, y out."""
+    return _create(_lib.OP_FORWARD, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+
+
+def create_cholesky_backward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
+                                                 dtype=torch.float64, device=None, stream=None,
+                                                 use_cuda_graph=False):
+    """Backward sweep on a stored factor; x: y in, solution out."""
+    return _create(_lib.OP_BACKWARD, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+
+
+def create_cholesky_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
+                                 dtype=torch.float64, device=None, stream=None,
+                                 use_cuda_graph=False):
+    """Forward then backward sweep on a stored factor; x: b in, solution out."""
+    return _create(_lib.OP_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
