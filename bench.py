@@ -1,0 +1,325 @@
+"""Benchmark: batched solves/s of the mixed-precision + FP64-refinement solver
+versus the plain FP64 path, at normwise relative backward error <= 1e-12.
+
+Workload: N=1024 blocks, n=64, m=8 right-hand sides, diagonal shift s=10,
+one system per GPU (README generator, seeded).  A step is one full solve of
+that system from its original blocks: float factor + refinement for the
+headline value, FP64 factor_and_solve for the comparison line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank solves its own replica (the path does not shard);
+value = systems solved by all ranks / max-over-ranks time.  The reference arm
+times the CPU oracle (NumPy restatement of the reference algorithm) on the
+host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BLOCKS, BLOCK, NRHS, SHIFT, SEED = 1024, 64, 8, 10.0, 0
+TOL, MAX_ITER = 1e-12, 10
+METRIC = "batched solves/s: mixed+refine vs plain FP64 on 1 B200 at rel. backward err <=1e-12"
+WORKLOAD = "N=1024 n=64 m=8 shift=10 single system per GPU (README generator, seed 0)"
+
+
+def storage_len(N):
+    return sum(N // (2 ** l) - 1 for l in range(N.bit_length()))
+
+
+def make_problem():
+    from oracle.generators import readme_problem
+    return readme_problem(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED)
+
+
+def algorithmic_factor_flops(N, n):
+    """Nested-dissection factor flop count: per level, potrf n^3/3 per node,
+    trsm n^3 per coupling side, syrk n^3 per coupling side, fill-in gemm 2 n^3."""
+    s, total = 1, 0.0
+    for _ in range(N.bit_length()):
+        d = (N + s) // (2 * s)
+        nodes = [s - 1 + 2 * s * t for t in range(d)]
+        r = sum(1 for i in nodes if i + s < N)
+        lft = sum(1 for i in nodes if i >= s)
+        both = sum(1 for i in nodes if i + s < N and i >= s)
+        total += d * n ** 3 / 3 + 2 * (r + lft) * n ** 3 + both * 2 * n ** 3
+        s *= 2
+    return total
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port (NumPy restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+def cpu_oracle_solves_per_s(L, E, b, reps):
+    from oracle import nd_cholesky as nd
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        nd.nd_factor_and_solve(L, E, b)
+        ts.append(time.perf_counter() - t0)
+    return 1.0 / statistics.median(ts), ts
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    L, E, b = make_problem()
+    cores = len(os.sched_getaffinity(0))
+    from oracle import nd_cholesky as nd
+    for _ in range(args.warmup):
+        nd.nd_factor_and_solve(L, E, b)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, _, x = nd.nd_factor_and_solve(L, E, b)
+        ts.append(time.perf_counter() - t0)
+    eta = float(nd.backward_error(L, E, x, b)[0])
+    sec = statistics.mean(ts)
+    value = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "N": N_BLOCKS, "n": BLOCK, "m": NRHS, "shift": SHIFT,
+                   "l2": "host CPU run"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "one full FP64 factor_and_solve of the workload system per step "
+                                   "(NumPy oracle restating socu's level loop; BLAS threads = host cores)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "backward_error": eta,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from socu_b200.block_tridiag_solver import create_cholesky_factor_and_solve_launch, create_cholesky_factor_launch
+    from socu_b200.mixed import backward_error, create_cholesky_refined_solve_launch
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    L_np, E_np, b_np = make_problem()
+    L0 = torch.tensor(L_np, device=dev)
+    E0 = torch.tensor(E_np, device=dev)
+    b0 = torch.tensor(b_np, device=dev)
+    x = torch.zeros_like(b0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # mixed + refinement (headline), inputs read-only
+    mixed = create_cholesky_refined_solve_launch(L0, E0, b0, x, tol=TOL, max_iter=MAX_ITER, use_cuda_graph=True)
+    # plain FP64 factor_and_solve on working copies (in place)
+    Lw, Ew, xw = L0.clone(), E0.clone(), b0.clone()
+    plain = create_cholesky_factor_and_solve_launch(Lw, Ew, xw, use_cuda_graph=True)
+    # float factor alone, for the dominant-phase roofline
+    L32, E32 = L0.float(), E0.float()
+    L32w, E32w = L32.clone(), E32.clone()
+    fac32 = create_cholesky_factor_launch(L32w, E32w, dtype=torch.float32, use_cuda_graph=True)
+
+    def time_steps(fn, reset, k):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for a, bev in evs:
+            reset()
+            flush.zero_()
+            a.record()
+            fn()
+            bev.record()
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(bev) * 1e-3 for a, bev in evs]
+
+    def reset_plain():
+        Lw.copy_(L0); Ew.copy_(E0); xw.copy_(b0)
+
+    def reset_fac():
+        L32w.copy_(L32); E32w.copy_(E32)
+
+    nothing = lambda: None
+    for _ in range(args.warmup):
+        mixed(); reset_plain(); plain(); reset_fac(); fac32()
+    barrier()
+
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        barrier()
+        t_mixed = time_steps(mixed, nothing, args.steps)
+        barrier()
+    t_plain = time_steps(plain, reset_plain, args.steps)
+    t_fac = time_steps(fac32, reset_fac, args.steps)
+    barrier()
+
+    eta_dev = float(mixed.eta.max())
+    iters = int(mixed.iterations.max())
+    eta_check = float(backward_error(L0, E0, x, b0).max())
+    x_plain = xw.clone()
+    eta_plain = float(backward_error(L0, E0, x_plain, b0).max())
+
+    # e2e through the public API with host buffers (pinned), copies inside the timed region
+    Lh = L0.cpu().pin_memory(); Eh = E0.cpu().pin_memory(); bh = b0.cpu().pin_memory()
+    xh = torch.empty_like(x, device="cpu").pin_memory()
+    Ld, Ed, bd, xd = torch.empty_like(L0), torch.empty_like(E0), torch.empty_like(b0), torch.empty_like(b0)
+    e2e_run = create_cholesky_refined_solve_launch(Ld, Ed, bd, xd, tol=TOL, max_iter=MAX_ITER, use_cuda_graph=True)
+
+    def e2e_step():
+        Ld.copy_(Lh, non_blocking=True); Ed.copy_(Eh, non_blocking=True); bd.copy_(bh, non_blocking=True)
+        e2e_run()
+        xh.copy_(xd, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    t_e2e = time_steps(e2e_step, nothing, max(3, args.steps // 2))
+    h2d = Lh.numel() * 8 + Eh.numel() * 8 + bh.numel() * 8
+    d2h = xh.numel() * 8
+
+    def agg(ts):
+        v = torch.tensor([statistics.mean(ts)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        return float(v)
+
+    sec_mixed, sec_plain, sec_fac, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_fac), agg(t_e2e)
+    if rank != 0:
+        return
+    n, N, m = BLOCK, N_BLOCKS, NRHS
+    S = storage_len(N)
+    fac_bytes = 2.0 * (N + S) * n * n * 4   # read + write the float L and E once
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        hbm_peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    achieved = fac_bytes / sec_fac / 1e9
+    cores = len(os.sched_getaffinity(0))
+    cpu_v, cpu_ts = cpu_oracle_solves_per_s(L_np, E_np, b_np, reps=2)
+    value = world / sec_mixed
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec_mixed * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor + f64 refinement", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "N": N, "n": n, "m": m, "shift": SHIFT, "tol": TOL,
+                   "max_iter": MAX_ITER, "l2": "256 MB flush before every timed step",
+                   "parallelism": f"replicas x{world} (one system per GPU)"},
+        "fp64_plain": {"value": world / sec_plain, "unit": "solves/s", "ms_per_step": sec_plain * 1e3,
+                       "backward_error": eta_plain},
+        "mixed_over_fp64": sec_plain / sec_mixed,
+        "backward_error": {"max": eta_dev, "recomputed": eta_check, "iterations": iters},
+        "factor_flops_fp": algorithmic_factor_flops(N, n),
+        "roofline": {"kernel": "float factor (k_node + k_update per level)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "peak_source": peak_src, "traffic": None,
+                     "algorithmic_bytes": fac_bytes, "ms_per_launch": sec_fac * 1e3},
+        "cpu_baseline": {"value": cpu_v, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "one FP64 factor_and_solve of the workload system, median of 2 "
+                                   f"({[round(t, 3) for t in cpu_ts]} s)"},
+        "e2e": {"value": world / sec_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": sec_e2e * 1e3},
+        "gpu_launches": mixed.kernel_count * args.steps,
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -108,6 +108,34 @@ int64_t socu_launch_kernel_count(socu_launch_t launch);
 
 int socu_launch_destroy(socu_launch_t launch);
 
+/* ---- mixed precision with FP64 iterative refinement (no counterpart in the
+ * reference, which only has plain f32/f64 paths) ----
+ * Solves Psi x = b for FP64 inputs: a float copy of (L, E) is factored with the
+ * same nested-dissection kernels, then x is refined in FP64 against the
+ * original blocks until the normwise backward error
+ *     eta = ||b - Psi x||_inf / (||Psi||_inf ||x||_inf + ||b||_inf) <= tol
+ * or max_iter corrections were applied.  L, E and b are not modified.
+ * eta (batch,) and iters (batch,) are device outputs; iters < 0 flags a
+ * non-finite residual (float factor broke down) after -iters steps.
+ * The workspace (>= socu_refine_workspace_bytes, 256-byte aligned device
+ * memory) is owned by the caller; nothing is allocated here. */
+size_t socu_refine_workspace_bytes(int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs);
+
+int socu_refine_solve(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
+                      int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
+                      void* workspace, size_t workspace_bytes, double* eta, int32_t* iters, void* stream);
+
+/* Launch object for socu_refine_solve (buffers bound; optional CUDA graph). */
+int socu_refine_launch_create(socu_launch_t* out, const double* L, const double* E, const double* b, double* x,
+                              const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
+                              int max_iter, double tol, void* workspace, size_t workspace_bytes, double* eta,
+                              int32_t* iters, int use_cuda_graph, void* stream);
+
+/* r = b - Psi x in FP64 against the original blocks (no counterpart in the
+ * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */
+int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,
+                                int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

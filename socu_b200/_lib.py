@@ -56,6 +56,12 @@ _SIGNATURES = {
     "socu_launch_run": (_int, [_vp, _vp]),
     "socu_launch_kernel_count": (_i64, [_vp]),
     "socu_launch_destroy": (_int, [_vp]),
+    "socu_refine_workspace_bytes": (ctypes.c_size_t, [_i64, _i64, _i64, _i64]),
+    "socu_refine_solve": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,
+                                 _vp, ctypes.c_size_t, _vp, _vp, _vp]),
+    "socu_refine_launch_create": (_int, [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64,
+                                         _int, ctypes.c_double, _vp, ctypes.c_size_t, _vp, _vp, _int, _vp]),
+    "socu_block_tridiag_residual": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
 }
 
 

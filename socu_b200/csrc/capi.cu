@@ -11,7 +11,7 @@
 #include <vector>
 
 #include "../../include/socu_b200.h"
-#include "nd_kernels.cuh"
+#include "refine.cuh"
 
 namespace socu {
 namespace {
@@ -27,7 +27,7 @@ int cuda_status(cudaError_t e) {
 std::vector<Level> schedule(int N) {
   // socu/block_tridiag_solver.py:869-914
   std::vector<Level> out;
-  int s = 1, curr = 0, nxt = N - 1;
+  int s = 1, prev = 0, curr = 0, nxt = N - 1;
   const int K = static_cast<int>(socu_recursive_iterations(N));
   for (int l = 0; l < K; ++l) {
     Level lv;
@@ -35,8 +35,10 @@ std::vector<Level> schedule(int N) {
     lv.d = (N + s) / (2 * s);
     lv.oc = curr;
     lv.on = nxt;
+    lv.op = prev;
     out.push_back(lv);
     s *= 2;
+    prev = curr;
     curr = nxt;
     nxt += N / s - 1;
   }
@@ -123,58 +125,58 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count) 
   const int K = static_cast<int>(lv.size());
   const int n = p.n, nth = threads_for(n);
   const bool withY = op == SOCU_OP_FACTOR_AND_SOLVE;
-  const size_t sd = smem_diag_elems(n, withY ? p.m : 0) * sizeof(T);
-  const size_t sc = smem_couple_elems(n) * sizeof(T);
-  const size_t su = smem_update_elems(n) * sizeof(T);
-  const size_t ss = smem_sweep_elems(n, p.m > 0 ? p.m : 1) * sizeof(T);
+  const size_t sd = smem_node_elems(n, sizeof(T)) * sizeof(T);
+  const size_t su = smem_update_elems(n, sizeof(T)) * sizeof(T);
+  const int mm = p.m > 0 ? p.m : 1;
+  const bool res = (long long)smem_sweep_res_elems(n, mm) * (long long)sizeof(T) <= (long long)max_smem_optin();
+  const size_t ss = (res ? smem_sweep_res_elems(n, mm) : smem_sweep_elems(n, mm)) * sizeof(T);
   const int nt = ceil_div(n, kTile), nlt = nt * (nt + 1) / 2;
+  auto node_kernel = withY ? k_node<T, true> : k_node<T, false>;
+  auto fwd_kernel = res ? k_fwd<T, true> : k_fwd<T, false>;
+  auto pull_kernel = res ? k_fwd<T, true, true> : k_fwd<T, false, true>;
+  auto bwd_kernel = res ? k_bwd<T, true> : k_bwd<T, false>;
   long long launches = 0;
   const bool run = count == nullptr;
 
   if (run) {
     cudaError_t e = cudaSuccess;
     if (op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE) {
-      e = withY ? prepare(k_diag<T, true>, sd) : prepare(k_diag<T, false>, sd);
-      if (e == cudaSuccess) e = prepare(k_couple<T>, sc);
+      e = prepare(node_kernel, sd);
       if (e == cudaSuccess) e = prepare(k_update<T>, su);
     }
-    if (e == cudaSuccess) e = prepare(k_fwd_node<T>, ss);
-    if (e == cudaSuccess) e = prepare(k_fwd_update<T>, ss);
-    if (e == cudaSuccess) e = prepare(k_bwd<T>, ss);
+    if (e == cudaSuccess) e = prepare(fwd_kernel, ss);
+    if (e == cudaSuccess) e = prepare(pull_kernel, ss);
+    if (e == cudaSuccess) e = prepare(bwd_kernel, ss);
     if (e != cudaSuccess) return cuda_status(e);
   }
 
-  auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L) {
+  auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
     if (blocks <= 0) return;
     ++launches;
-    if (run) kernel<<<(unsigned)blocks, nth, smem, st>>>(p, L);
+    if (run) kernel<<<(unsigned)blocks, threads > 0 ? threads : nth, smem, st>>>(p, L);
   };
 
   const bool factor = op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (factor) {
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
-      if (withY)
-        go(k_diag<T, true>, (long long)p.B * L.d, sd, L);
-      else
-        go(k_diag<T, false>, (long long)p.B * L.d, sd, L);
+      go(node_kernel, (long long)p.B * L.d, sd, L, 256);
       if (l + 1 < K) {
-        go(k_couple<T>, (long long)p.B * L.d * 2 * nt, sc, L);
         const int U = p.N / (2 * L.s);
         go(k_update<T>, (long long)p.B * (U * nlt + (L.d - 1) * nt * nt), su, L);
-        if (withY) go(k_fwd_update<T>, (long long)p.B * U, ss, L);
+        // fused forward: apply this level's updates to every target vector
+        if (withY) go(pull_kernel, (long long)p.B * (p.N / lv[l + 1].s), ss, lv[l + 1]);
       }
     }
   }
   if (op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE) {
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
-      go(k_fwd_node<T>, (long long)p.B * L.d, ss, L);
-      if (l + 1 < K) go(k_fwd_update<T>, (long long)p.B * (p.N / (2 * L.s)), ss, L);
+      go(fwd_kernel, (long long)p.B * (l == 0 ? L.d : p.N / L.s), ss, L);
     }
   }
   if (op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE) {
-    for (int l = K - 1; l >= 0; --l) go(k_bwd<T>, (long long)p.B * lv[l].d, ss, lv[l]);
+    for (int l = K - 1; l >= 0; --l) go(bwd_kernel, (long long)p.B * lv[l].d, ss, lv[l]);
   }
   if (count) *count = launches;
   if (run) return cuda_status(cudaGetLastError());
@@ -204,7 +206,8 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
   d->S = (int)S;
   // grid sizes of the widest launches must fit
   const int nt = ceil_div(d->n, kTile);
-  const long long widest = (long long)d->B * ((d->N + 1) / 2) * 2 * nt * nt + 1;
+  const long long per_node = 2LL * nt * nt + 1;
+  const long long widest = (long long)d->B * ((d->N + 1) / 2) * per_node + 1;
   if (!grid_ok(widest)) return SOCU_ERR_UNSUPPORTED;
   return SOCU_OK;
 }
@@ -228,6 +231,106 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
   return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count);
 }
 
+
+// ---------------------------------------------------------------------------
+// mixed precision + FP64 refinement
+// ---------------------------------------------------------------------------
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct RefineLayout {
+  size_t l32, e32, r32, active, state, any, total;
+};
+
+RefineLayout refine_layout(int64_t B, int64_t N, int64_t n, int64_t m) {
+  RefineLayout o;
+  const int64_t S = socu_off_diag_storage_len(N);
+  size_t off = 0;
+  o.l32 = off; off += align256((size_t)B * N * n * n * sizeof(float));
+  o.e32 = off; off += align256((size_t)B * (S > 0 ? S : 0) * n * n * sizeof(float));
+  o.r32 = off; off += align256((size_t)B * N * n * m * sizeof(float));
+  o.active = off; off += align256((size_t)B);
+  o.state = off; off += align256((size_t)B * sizeof(RefineState));
+  o.any = off; off += align256(sizeof(int));
+  o.total = off;
+  return o;
+}
+
+int refine_validate(const void* L, const void* E, const void* b, void* x, int64_t batch, int64_t horizon,
+                    int64_t n, int64_t n_rhs, int max_iter, double tol, void* ws, size_t ws_bytes,
+                    const double* eta, const int32_t* iters, Dims* d) {
+  const int v = validate(SOCU_OP_SOLVE, SOCU_FLOAT32, L, E, x, batch, horizon, n, n_rhs, d);
+  if (v != SOCU_OK) return v;
+  if (max_iter < 1 || max_iter > 1000 || !(tol >= 0.0)) return SOCU_ERR_INVALID_ARGUMENT;
+  if (batch > 0 && (b == nullptr || eta == nullptr || iters == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
+  if ((long long)smem_residual_elems(d->n) * (long long)sizeof(double) > (long long)max_smem_optin())
+    return SOCU_ERR_UNSUPPORTED;
+  const RefineLayout lay = refine_layout(batch, horizon, n, n_rhs);
+  if (batch > 0 && (ws == nullptr || ws_bytes < lay.total || (reinterpret_cast<uintptr_t>(ws) & 255) != 0))
+    return SOCU_ERR_INVALID_ARGUMENT;
+  return SOCU_OK;
+}
+
+RefineArgs refine_args(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
+                       const Dims& d, int max_iter, double tol, void* ws, double* eta, int32_t* iters) {
+  const RefineLayout lay = refine_layout(d.B, d.N, d.n, d.m);
+  char* w = static_cast<char*>(ws);
+  RefineArgs a;
+  a.L = L; a.E = E; a.b = b; a.x = x; a.mask = mask;
+  a.L32 = reinterpret_cast<float*>(w + lay.l32);
+  a.E32 = reinterpret_cast<float*>(w + lay.e32);
+  a.R32 = reinterpret_cast<float*>(w + lay.r32);
+  a.active = reinterpret_cast<uint8_t*>(w + lay.active);
+  a.st = reinterpret_cast<RefineState*>(w + lay.state);
+  a.any_active = reinterpret_cast<int*>(w + lay.any);
+  a.eta = eta; a.iters = iters; a.rout = nullptr;
+  a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
+  a.tol = tol; a.max_iter = max_iter;
+  return a;
+}
+
+// Enqueue (or count) the full mixed solve: init, float factor, max_iter x
+// (float solve, x update, FP64 residual, check).
+int refine_enqueue(const RefineArgs& a, cudaStream_t st, long long* count) {
+  const bool run = count == nullptr;
+  long long launches = 0;
+  Dims d{a.B, a.N, a.n, a.m, a.S};
+  Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
+  Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
+  const int nrc = ceil_div(a.n, kResRows);
+  const size_t sres = smem_residual_elems(a.n) * sizeof(double);
+  const long long nvec = (long long)a.B * a.N * a.n * a.m;
+  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
+  const int chk_blocks = (a.B + 255) / 256;
+  if (run) {
+    cudaError_t e = prepare(k_residual<true>, sres);
+    if (e != cudaSuccess) return cuda_status(e);
+    k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
+    k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+  }
+  launches += 2;
+  long long c = 0;
+  int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c);
+  if (s != SOCU_OK) return s;
+  launches += run ? 0 : c;
+  long long cs = 0;
+  if (!run) {
+    s = enqueue<float>(SOCU_OP_SOLVE, pf, nullptr, &cs);
+    if (s != SOCU_OK) return s;
+  }
+  for (int it = 0; it < a.max_iter; ++it) {
+    if (run) {
+      s = enqueue<float>(SOCU_OP_SOLVE, pf, st, nullptr);
+      if (s != SOCU_OK) return s;
+      k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+      k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
+    }
+    launches += cs + 3;
+  }
+  if (count) *count = launches;
+  if (run) return cuda_status(cudaGetLastError());
+  return SOCU_OK;
+}
 }  // namespace
 }  // namespace socu
 
@@ -242,7 +345,51 @@ struct socu_launch_s {
   long long kernels;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
+  bool refine = false;
+  RefineArgs ra{};
 };
+
+namespace {
+// enqueue one run of a launch object on `st`
+int launch_enqueue(socu_launch_s* h, cudaStream_t st) {
+  if (h->refine) {
+    if (h->batch == 0) return SOCU_OK;
+    const cudaError_t e = ensure_device(h->L);
+    if (e != cudaSuccess) return cuda_status(e);
+    return refine_enqueue(h->ra, st, nullptr);
+  }
+  return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st, nullptr);
+}
+
+// Capture one run into a CUDA graph on a private stream (the legacy default
+// stream cannot capture) and instantiate it eagerly.
+int capture(socu_launch_s* h) {
+  const cudaError_t ed = ensure_device(h->L);
+  if (ed != cudaSuccess) return cuda_status(ed);
+  cudaStream_t cap = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+  int st = SOCU_OK;
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = launch_enqueue(h, cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+    if (st == SOCU_OK && e2 != cudaSuccess) st = cuda_status(e2);
+    h->graph = g;
+    if (st == SOCU_OK) st = cuda_status(cudaGraphInstantiate(&h->exec, g, 0));
+  } else {
+    st = cuda_status(e);
+  }
+  if (cap) cudaStreamDestroy(cap);
+  if (st != SOCU_OK) {
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->exec = nullptr;
+    h->graph = nullptr;
+  }
+  return st;
+}
+}  // namespace
 
 extern "C" {
 
@@ -285,12 +432,11 @@ int64_t socu_max_block_size(socu_dtype dtype, int64_t n_rhs) {
   const long long limit = max_smem_optin();
   int64_t best = 0;
   for (int n = 1; n <= 512; ++n) {
-    long long need = smem_diag_elems(n, m);
-    const long long c = smem_couple_elems(n), u = smem_update_elems(n), s = smem_sweep_elems(n, m > 0 ? m : 1);
-    if (c > need) need = c;
+    long long need = smem_node_elems(n, (int)es);
+    const long long u = smem_update_elems(n, (int)es), s = smem_sweep_elems(n, m > 0 ? m : 1);
     if (u > need) need = u;
     if (s > need) need = s;
-    if (need * (long long)es <= limit) best = n;
+    if (need * (long long)es <= limit && n <= 128) best = n;
   }
   return best;
 }
@@ -352,35 +498,13 @@ int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L
   h->graph = nullptr;
   h->exec = nullptr;
   if (use_cuda_graph && batch > 0) {
-    const cudaError_t ed = ensure_device(L);
-    if (ed != cudaSuccess) {
-      delete h;
-      return cuda_status(ed);
-    }
-    // Capture on a private stream (the legacy default stream cannot capture),
-    // then instantiate eagerly so the first run is a single graph launch.
-    cudaStream_t cap = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      st = dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, cap, nullptr);
-      cudaGraph_t g = nullptr;
-      const cudaError_t e2 = cudaStreamEndCapture(cap, &g);
-      if (st == SOCU_OK && e2 != cudaSuccess) st = cuda_status(e2);
-      h->graph = g;
-      if (st == SOCU_OK) st = cuda_status(cudaGraphInstantiate(&h->exec, g, 0));
-    } else {
-      st = cuda_status(e);
-    }
-    if (cap) cudaStreamDestroy(cap);
+    st = capture(h);
     if (st != SOCU_OK) {
-      if (h->exec) cudaGraphExecDestroy(h->exec);
-      if (h->graph) cudaGraphDestroy(h->graph);
       delete h;
       return st;
     }
-    (void)stream;
   }
+  (void)stream;
   *out = h;
   return SOCU_OK;
 }
@@ -389,11 +513,91 @@ int socu_launch_run(socu_launch_t h, void* stream) {
   if (h == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (h->exec) return cuda_status(cudaGraphLaunch(h->exec, st));
-  return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st,
-                  nullptr);
+  return launch_enqueue(h, st);
 }
 
 int64_t socu_launch_kernel_count(socu_launch_t h) { return h ? h->kernels : 0; }
+
+size_t socu_refine_workspace_bytes(int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs) {
+  if (batch < 0 || horizon <= 0 || n <= 0 || n_rhs <= 0) return 0;
+  return refine_layout(batch, horizon, n, n_rhs).total;
+}
+
+int socu_refine_solve(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
+                      int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
+                      void* workspace, size_t workspace_bytes, double* eta, int32_t* iters, void* stream) {
+  Dims d;
+  int v = refine_validate(L, E, b, x, batch, horizon, n, n_rhs, max_iter, tol, workspace, workspace_bytes, eta,
+                          iters, &d);
+  if (v != SOCU_OK || batch == 0) return v;
+  const cudaError_t e = ensure_device(L);
+  if (e != cudaSuccess) return cuda_status(e);
+  const RefineArgs a = refine_args(L, E, b, x, mask, d, max_iter, tol, workspace, eta, iters);
+  return refine_enqueue(a, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,
+                                int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream) {
+  Dims d;
+  int v = validate(SOCU_OP_SOLVE, SOCU_FLOAT64, L, E, x, batch, horizon, n, n_rhs, &d);
+  if (v != SOCU_OK) return v;
+  if (batch == 0) return SOCU_OK;
+  if (b == nullptr || r == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  if ((long long)smem_residual_elems(d.n) * (long long)sizeof(double) > (long long)max_smem_optin())
+    return SOCU_ERR_UNSUPPORTED;
+  cudaError_t e = ensure_device(L);
+  if (e != cudaSuccess) return cuda_status(e);
+  RefineArgs a{};
+  a.L = L; a.E = E; a.b = b; a.x = const_cast<double*>(x); a.rout = r;
+  a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
+  const size_t sres = smem_residual_elems(d.n) * sizeof(double);
+  e = prepare(k_residual<false>, sres);
+  if (e != cudaSuccess) return cuda_status(e);
+  const int nrc = ceil_div(d.n, kResRows);
+  k_residual<false><<<(unsigned)((long long)d.B * d.N * nrc), 256, sres, static_cast<cudaStream_t>(stream)>>>(a);
+  return cuda_status(cudaGetLastError());
+}
+
+int socu_refine_launch_create(socu_launch_t* out, const double* L, const double* E, const double* b, double* x,
+                              const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
+                              int max_iter, double tol, void* workspace, size_t workspace_bytes, double* eta,
+                              int32_t* iters, int use_cuda_graph, void* stream) {
+  if (out == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  Dims d;
+  int st = refine_validate(L, E, b, x, batch, horizon, n, n_rhs, max_iter, tol, workspace, workspace_bytes, eta,
+                           iters, &d);
+  if (st != SOCU_OK) return st;
+  socu_launch_s* h = new (std::nothrow) socu_launch_s();
+  if (!h) return SOCU_ERR_UNSUPPORTED;
+  h->op = SOCU_OP_SOLVE;
+  h->dtype = SOCU_FLOAT64;
+  h->L = const_cast<double*>(L);
+  h->E = const_cast<double*>(E);
+  h->x = x;
+  h->mask = mask;
+  h->batch = batch;
+  h->horizon = horizon;
+  h->n = n;
+  h->n_rhs = n_rhs;
+  h->graph = nullptr;
+  h->exec = nullptr;
+  h->refine = true;
+  h->ra = batch > 0 ? refine_args(L, E, b, x, mask, d, max_iter, tol, workspace, eta, iters) : RefineArgs{};
+  long long kernels = 0;
+  if (batch > 0) refine_enqueue(h->ra, nullptr, &kernels);
+  h->kernels = kernels;
+  if (use_cuda_graph && batch > 0) {
+    st = capture(h);
+    if (st != SOCU_OK) {
+      delete h;
+      return st;
+    }
+  }
+  (void)stream;
+  *out = h;
+  return SOCU_OK;
+}
 
 int socu_launch_destroy(socu_launch_t h) {
   if (h == nullptr) return SOCU_OK;

@@ -9,11 +9,9 @@
 // (socu/block_tridiag_solver.py:174).  Slot E[o_l + k] couples node
 // p = (k+1)s-1 (columns) with q = p+s (rows).
 //
-// After a factor the upper triangle of every L block holds the strictly
-// upper part of C^{-T} (C = lower Cholesky factor of that block).  The
-// reference leaves that triangle unspecified; the substitution sweeps here
-// only ever read the lower triangle, so factors are interchangeable with the
-// reference's.
+// Factor output: lower(L_i) = C_i (lower Cholesky factor), upper(L_i) = 0.
+// The reference leaves the upper triangle unspecified; every kernel here reads
+// only lower(L_i), so factors are interchangeable with socu's.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -21,11 +19,12 @@
 
 namespace socu {
 
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBS = 32;  // row block of the blocked triangular solves
+
 template <typename T> __device__ __forceinline__ T rsqrt_t(T x);
 template <> __device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
 template <> __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
-
-template <typename T> __device__ __forceinline__ T rcp_t(T x) { return T(1) / x; }
 
 template <typename T>
 struct Problem {
@@ -54,34 +53,134 @@ struct Level {
   int d;    // nodes at this level, (N+s)/(2s)
   int oc;   // offset of this level's slots
   int on;   // offset of the next level's slots
+  int op;   // offset of the previous level's slots (unused at level 0)
 };
 
 // ---------------------------------------------------------------------------
-// Register-tiled CTA GEMM on accessor functors.
-//   acc(r,c) = sum_k a(r,k) * b(k,c) for 0<=r<M, 0<=c<N, k in [k0(r0,c0), K)
-//   then out(r, c, acc) for every valid entry (and c <= r if LOWER).
-// Threads own TM x TN micro-tiles; consecutive threads own consecutive
-// column tiles so that row operands are broadcast within a warp.
+// Asynchronous global -> shared copies (cp.async, element granular so that
+// padded shared layouts are allowed).  Issue everything, then wait once.
 // ---------------------------------------------------------------------------
-template <typename T, int TM, int TN, bool LOWER, class FA, class FB, class FO>
-__device__ __forceinline__ void cta_gemm(int M, int N, int K, FA a, FB b, FO out) {
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_bytes(void* dst, const void* src) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
+  cp_async_bytes<sizeof(T)>(dst, src);
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// widest copy (16, 8 or element bytes) that keeps every row chunk aligned
+template <typename T>
+__device__ __forceinline__ int copy_width(const T* dst, int ld, const T* src, int cols, long long src_ld) {
+  const unsigned long long a = reinterpret_cast<unsigned long long>(src) |
+                               (unsigned long long)smem_addr(dst) |
+                               (unsigned long long)(cols * sizeof(T)) | (unsigned long long)(ld * sizeof(T)) |
+                               (unsigned long long)(src_ld * (long long)sizeof(T));
+  return (a & 15) == 0 ? 16 : ((a & 7) == 0 ? 8 : (int)sizeof(T));
+}
+
+template <typename T, int BYTES>
+__device__ __forceinline__ void async_load_w(T* dst, int ld, const T* src, int rows, int cols, long long src_ld) {
+  constexpr int V = BYTES / sizeof(T);
+  const int cv = cols / V;
+  const int total = rows * cv;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int r = e / cv, c = (e - r * cv) * V;
+    cp_async_bytes<BYTES>(dst + r * ld + c, src + (long long)r * src_ld + c);
+  }
+}
+
+// dst[r*ld + c] = src[r*src_ld + c]; vectorised when alignment allows
+template <typename T>
+__device__ __forceinline__ void async_load(T* dst, int ld, const T* src, int rows, int cols, long long src_ld) {
+  const int w = copy_width(dst, ld, src, cols, src_ld);
+  if (w == 16)
+    async_load_w<T, 16>(dst, ld, src, rows, cols, src_ld);
+  else if (w == 8)
+    async_load_w<T, 8>(dst, ld, src, rows, cols, src_ld);
+  else
+    async_load_w<T, sizeof(T)>(dst, ld, src, rows, cols, src_ld);
+}
+
+// dst[c*ld + r] = src[r*src_ld + c]   (global rows become shared columns)
+template <typename T>
+__device__ __forceinline__ void async_load_t(T* dst, int ld, const T* src, int rows, int cols, long long src_ld) {
+  const int total = rows * cols;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int r = e / cols, c = e - r * cols;
+    cp_async_elem(dst + c * ld + r, src + (long long)r * src_ld + c);
+  }
+}
+
+// even leading dimension (row starts 8/16-byte aligned) close to n
+__host__ __device__ inline int even_ld(int n) { return n + ((n & 1) ? 1 : 2); }
+
+template <typename T>
+__device__ __forceinline__ void store_block(T* dst, long long dst_ld, const T* src, int ld, int rows, int cols) {
+  const int total = rows * cols;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int r = e / cols, c = e - r * cols;
+    dst[(long long)r * dst_ld + c] = src[r * ld + c];
+  }
+}
+
+// dst[r*dst_ld + c] = src[c*ld + r]
+template <typename T>
+__device__ __forceinline__ void store_block_t(T* dst, long long dst_ld, const T* src, int ld, int rows, int cols) {
+  const int total = rows * cols;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int r = e / cols, c = e - r * cols;
+    dst[(long long)r * dst_ld + c] = src[c * ld + r];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Register-tiled CTA GEMM on shared-memory operands.
+//   acc(r,c) = sum_{k<K} opA(r,k) opB(k,c),  0<=r<M, 0<=c<N
+//   opA(r,k) = TA ? A[k*lda + r] : A[r*lda + k]
+//   opB(k,c) = TB ? B[c*ldb + k] : B[k*ldb + c]
+// then out(r, c, acc) for every valid entry (c <= r only if LOWER).
+// Threads own TM x TN micro-tiles; consecutive threads take consecutive
+// column tiles so row operands are broadcast inside a warp.  Out-of-range
+// rows/columns are clamped for loading and masked on output, so the k-loop
+// carries no branches.
+// ---------------------------------------------------------------------------
+template <typename T, int TM, int TN, bool TA, bool TB, bool LOWER = false, class Out>
+__device__ __forceinline__ void smem_gemm(int M, int N, int K, const T* __restrict__ A, int lda,
+                                          const T* __restrict__ B, int ldb, Out out) {
   const int tm = (M + TM - 1) / TM;
   const int tn = (N + TN - 1) / TN;
   for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
     const int r0 = (t / tn) * TM;
     const int c0 = (t % tn) * TN;
     if (LOWER && c0 > r0 + TM - 1) continue;
+    int ra[TM], cb[TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) ra[i] = min(r0 + i, M - 1);
+#pragma unroll
+    for (int j = 0; j < TN; ++j) cb[j] = min(c0 + j, N - 1);
     T acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
       for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+#pragma unroll 4
     for (int k = 0; k < K; ++k) {
       T av[TM], bv[TN];
 #pragma unroll
-      for (int i = 0; i < TM; ++i) av[i] = (r0 + i < M) ? a(r0 + i, k) : T(0);
+      for (int i = 0; i < TM; ++i) av[i] = TA ? A[k * lda + ra[i]] : A[ra[i] * lda + k];
 #pragma unroll
-      for (int j = 0; j < TN; ++j) bv[j] = (c0 + j < N) ? b(k, c0 + j) : T(0);
+      for (int j = 0; j < TN; ++j) bv[j] = TB ? B[cb[j] * ldb + k] : B[k * ldb + cb[j]];
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -98,121 +197,174 @@ __device__ __forceinline__ void cta_gemm(int M, int N, int K, FA a, FB b, FO out
 }
 
 // ---------------------------------------------------------------------------
-// Global <-> shared block copies (row-major, contiguous rows of length cols).
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) warp GEMM on shared operands.
+//   acc(r,c) = sum_{k<K} opA(r,k) opB(k,c);  out(r, c, acc) per valid entry.
+// Warp tiles of 16 x 32 (2 x 4 mma tiles).  Fragment layouts (PTX ISA,
+// mma.m8n8k4 .f64): A a0 = A[g][t], B b0 = B[t][g], C {c0,c1} = C[g][2t+{0,1}]
+// with g = lane/4, t = lane%4.  Leading dimensions of 4 (mod 16) doubles make
+// every fragment load conflict-free.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void load_block(T* __restrict__ dst, int ld, const T* __restrict__ src,
-                                           int rows, int cols, int src_ld) {
-  const int total = rows * cols;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int r = e / cols, c = e - r * cols;
-    dst[r * ld + c] = src[(long long)r * src_ld + c];
-  }
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
 }
 
-template <typename T>
-__device__ __forceinline__ void store_block(T* __restrict__ dst, int dst_ld, const T* __restrict__ src,
-                                            int ld, int rows, int cols) {
-  const int total = rows * cols;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int r = e / cols, c = e - r * cols;
-    dst[(long long)r * dst_ld + c] = src[r * ld + c];
-  }
-}
+__host__ __device__ inline int ld_dmma(int n) { return ((n + 15) / 16) * 16 + 4; }
 
-// ---------------------------------------------------------------------------
-// One warp: in-place lower Cholesky of a kb x kb diagonal block (kb <= 32)
-// followed by the inverse of that factor.
-//   on exit: lower(A) = C, A[c*ld + r] = (C^{-1})[r][c] for r > c,
-//            dinv[r] = 1 / C[r][r].
-// Right-looking column steps; lane r owns row r.
-// ---------------------------------------------------------------------------
-template <typename T>
-__device__ void warp_chol_inv(T* A, int ld, int kb, T* dinv) {
-  const int lane = threadIdx.x & 31;
-  for (int j = 0; j < kb; ++j) {
-    const T ajj = A[j * ld + j];
-    const T rs = rsqrt_t(ajj);
-    if (lane > j && lane < kb) A[lane * ld + j] *= rs;
-    __syncwarp();
-    if (lane == j) {
-      A[j * ld + j] = ajj * rs;
-      dinv[j] = rs;
-    }
-    if (lane > j && lane < kb) {
-      const T lrj = A[lane * ld + j];
-      for (int c = j + 1; c <= lane; ++c) A[lane * ld + c] = fma(-lrj, A[c * ld + j], A[lane * ld + c]);
-    }
-    __syncwarp();
-  }
-  // inverse W = C^{-1} (lower); S[r][c] = sum_{k=c}^{r-1} C[r][k] W[k][c]
-  // accumulates in A[c*ld + r]; W[r][c] = -dinv[r] * S[r][c].
-  if (lane < kb)
-    for (int r = lane + 1; r < kb; ++r) A[lane * ld + r] = T(0);
-  __syncwarp();
-  for (int k = 0; k < kb; ++k) {
-    if (lane < k) A[lane * ld + k] = -dinv[k] * A[lane * ld + k];
-    __syncwarp();
-    if (lane <= k) {
-      const T wkc = (lane == k) ? dinv[k] : A[lane * ld + k];
-      for (int r = k + 1; r < kb; ++r) A[lane * ld + r] = fma(A[r * ld + k], wkc, A[lane * ld + r]);
-    }
-    __syncwarp();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// CTA: blocked right-looking Cholesky of the n x n block in A (lower read)
-// plus the full inverse of the factor.
-//   on exit: lower(A) = C, strict upper(A) = strict upper of C^{-T},
-//            dinv[r] = 1 / C[r][r].
-// P is scratch of n * BS elements.
-// ---------------------------------------------------------------------------
-template <typename T, int BS>
-__device__ void cta_chol_inv(T* A, int ld, int n, T* dinv, T* P) {
-  const int warp = threadIdx.x >> 5;
-  for (int K = 0; K < n; K += BS) {
-    const int kb = min(BS, n - K);
-    if (warp == 0) warp_chol_inv<T>(A + K * ld + K, ld, kb, dinv + K);
-    __syncthreads();
-    const int R0 = K + kb, rows = n - R0;
-    if (rows > 0) {
-      // panel: C[R0+r][K+c] = sum_{k<=c} A[R0+r][K+k] * W_KK[c][k]
-      cta_gemm<T, 2, 2, false>(
-          rows, kb, kb,
-          [&](int r, int k) { return A[(R0 + r) * ld + K + k]; },
-          [&](int k, int c) { return k < c ? A[(K + k) * ld + K + c] : (k == c ? dinv[K + c] : T(0)); },
-          [&](int r, int c, T v) { P[r * BS + c] = v; });
-      __syncthreads();
-      for (int e = threadIdx.x; e < rows * kb; e += blockDim.x) {
-        const int r = e / kb, c = e - r * kb;
-        A[(R0 + r) * ld + K + c] = P[r * BS + c];
+template <bool TA, bool TB, bool LOWER = false, class Out>
+__device__ __forceinline__ void warp_gemm_f64(int M, int N, int K, const double* __restrict__ A, int lda,
+                                              const double* __restrict__ B, int ldb, Out out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tm = (M + 15) / 16, tn = (N + 31) / 32;
+  for (int tile = warp; tile < tm * tn; tile += nw) {
+    const int r0 = (tile / tn) * 16, c0 = (tile % tn) * 32;
+    if (LOWER && c0 > r0 + 15) continue;
+    double acc[2][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    int ra[2], cb[4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) ra[i] = min(r0 + 8 * i + g, M - 1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cb[j] = min(c0 + 8 * j + g, N - 1);
+#pragma unroll 2
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + t;
+      const bool kv = k < K;
+      const int kc = kv ? k : K - 1;
+      double a[2], b[4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double v = TA ? A[kc * lda + ra[i]] : A[ra[i] * lda + kc];
+        a[i] = kv ? v : 0.0;
       }
-      // trailing: A[R0+r][R0+c] -= sum_k P[r][k] P[c][k]  (lower)
-      cta_gemm<T, 2, 2, true>(
-          rows, rows, kb,
-          [&](int r, int k) { return P[r * BS + k]; },
-          [&](int k, int c) { return P[c * BS + k]; },
-          [&](int r, int c, T v) { A[(R0 + r) * ld + R0 + c] -= v; });
-      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double v = TB ? B[cb[j] * ldb + kc] : B[kc * ldb + cb[j]];
+        b[j] = kv ? v : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = r0 + 8 * i + g, c = c0 + 8 * j + 2 * t + e;
+          if (r < M && c < N && (!LOWER || c <= r)) out(r, c, acc[i][j][e]);
+        }
   }
-  // off-diagonal blocks of W, block row by block row
-  for (int I = BS; I < n; I += BS) {
-    const int ib = min(BS, n - I);
-    // Tm[r][c] = sum_{k=c}^{I-1} C[I+r][k] W[k][c]
-    cta_gemm<T, 2, 2, false>(
-        ib, I, I,
-        [&](int r, int k) { return A[(I + r) * ld + k]; },
-        [&](int k, int c) { return k > c ? A[c * ld + k] : (k == c ? dinv[c] : T(0)); },
-        [&](int r, int c, T v) { P[r * I + c] = v; });
+}
+
+// Type-dispatching CTA GEMM: DMMA for double, 4x4 SIMT micro-tiles for float.
+template <typename T, bool TA, bool TB, bool LOWER = false, class Out>
+__device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restrict__ A, int lda,
+                                         const T* __restrict__ B, int ldb, Out out) {
+  if constexpr (sizeof(T) == 8)
+    warp_gemm_f64<TA, TB, LOWER>(M, N, K, A, lda, B, ldb, out);
+  else
+    smem_gemm<T, 4, 4, TA, TB, LOWER>(M, N, K, A, lda, B, ldb, out);
+}
+
+
+// ---------------------------------------------------------------------------
+// CTA: blocked right-looking Cholesky of the n x n block in A fused with the
+// solve C V = V for nv vectors (columns of V), by 8-column blocks.
+//   1. every thread loads the 8x8 diagonal block into registers and (when
+//      FACTOR) factors it redundantly: no communication on the critical chain;
+//   2. one thread per item solves against that block: each row of the panel
+//      below it (A21 <- A21 C11^{-T}) and each vector segment
+//      (V1 <- C11^{-1} V1) -- the same forward substitution;
+//   3. trailing updates A22 -= P P^T (lower) and V2 -= P V1 with
+//      P = the solved panel (tensor cores for double).
+// FACTOR = false re-runs the solve with an already factored lower(A) = C.
+// On exit lower(A) = C.  Two barriers per 8 columns.
+// ---------------------------------------------------------------------------
+template <typename T, bool FACTOR>
+__device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
+  constexpr int BK = 8;
+  for (int K = 0; K < n; K += BK) {
+    const int kb = min(BK, n - K);
+    const int R0 = K + kb, rows = FACTOR ? n - R0 : 0;
+    // 1. diagonal block in registers (identity-padded past kb)
+    T c[BK][BK], rsv[BK];
+#pragma unroll
+    for (int i = 0; i < BK; ++i)
+#pragma unroll
+      for (int j = 0; j <= i; ++j)
+        c[i][j] = (i < kb) ? A[(K + i) * lda + K + j] : (i == j ? T(1) : T(0));
+    if (FACTOR) {
+#pragma unroll
+      for (int j = 0; j < BK; ++j) {
+        const T r = rsqrt_t(c[j][j]);
+        rsv[j] = r;
+        c[j][j] *= r;
+#pragma unroll
+        for (int i = j + 1; i < BK; ++i) c[i][j] *= r;
+#pragma unroll
+        for (int i = j + 1; i < BK; ++i)
+#pragma unroll
+          for (int l = j + 1; l <= i; ++l) c[i][l] = fma(-c[i][j], c[l][j], c[i][l]);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < BK; ++j) rsv[j] = T(1) / c[j][j];
+    }
+    // 2. forward substitution of every item against the diagonal block
+    for (int it = threadIdx.x; it < rows + nv; it += blockDim.x) {
+      T* base;
+      int stride;
+      if (it < rows) {
+        base = A + (R0 + it) * lda + K;   // panel row: contiguous columns
+        stride = 1;
+      } else {
+        base = V + K * ldv + (it - rows); // vector segment: rows of V
+        stride = ldv;
+      }
+      T x[BK];
+#pragma unroll
+      for (int j = 0; j < BK; ++j) x[j] = j < kb ? base[j * stride] : T(0);
+#pragma unroll
+      for (int j = 0; j < BK; ++j) {
+#pragma unroll
+        for (int i = 0; i < j; ++i) x[j] = fma(-x[i], c[j][i], x[j]);
+        x[j] *= rsv[j];
+      }
+#pragma unroll
+      for (int j = 0; j < BK; ++j)
+        if (j < kb) base[j * stride] = x[j];
+    }
     __syncthreads();
-    // W[I+r][c] = - sum_{k<=r} W_II[r][k] Tm[k][c], stored at A[c*ld + I + r]
-    cta_gemm<T, 2, 2, false>(
-        ib, I, ib,
-        [&](int r, int k) { return k < r ? A[(I + k) * ld + I + r] : (k == r ? dinv[I + r] : T(0)); },
-        [&](int k, int c) { return P[k * I + c]; },
-        [&](int r, int c, T v) { A[c * ld + I + r] = -v; });
+    // 3. write the factored diagonal block, then the trailing updates
+    if (FACTOR && threadIdx.x < BK * BK) {
+      const int i = threadIdx.x / BK, j = threadIdx.x % BK;
+      if (i < kb && j <= i) {
+        T v = T(0);
+#pragma unroll
+        for (int ii = 0; ii < BK; ++ii)
+#pragma unroll
+          for (int jj = 0; jj <= ii; ++jj)
+            if (ii == i && jj == j) v = c[ii][jj];
+        A[(K + i) * lda + K + j] = v;
+      }
+    }
+    if (R0 < n) {
+      const T* P = A + R0 * lda + K;
+      if (FACTOR)
+        cta_gemm<T, false, true, true>(n - R0, n - R0, kb, P, lda, P, lda,
+                                       [&](int r, int cc, T v) { A[(R0 + r) * lda + R0 + cc] -= v; });
+      if (nv > 0)
+        cta_gemm<T, false, false>(n - R0, nv, kb, P, lda, V + K * ldv, ldv,
+                                  [&](int r, int cc, T v) { V[(R0 + r) * ldv + cc] -= v; });
+    }
     __syncthreads();
   }
 }

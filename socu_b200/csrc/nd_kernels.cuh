@@ -1,145 +1,118 @@
 // Per-level kernels of the nested-dissection block-tridiagonal Cholesky.
 //
-// One factor level l (stride s) is three launches, all deterministic (no
+// One factor level l (stride s) is two launches, all deterministic (no
 // floating-point atomics, every output block has exactly one writer):
-//   k_diag    one CTA per level node i: C_i = chol(L_i) and C_i^{-1}
-//             (socu: potrf K2, block_tridiag_solver.py:197-216).  With a RHS it
-//             also applies y_i <- C_i^{-1} y_i (fused forward step, :108-110).
-//   k_couple  one CTA per (node, side, 32-row/col panel):
-//             right  F = E[o_l + i/s] C_i^{-T}        (trsm_rltn K3, :219-248)
-//             left   G = C_i^{-1} E[o_l + (i-s)/s]    (trsm_llnn K4, :251-279)
-//             both as GEMMs against the stored inverse.
+//   k_node    one CTA per level node i: C_i = chol(L_i) in place
+//             (socu: potrf K2, block_tridiag_solver.py:197-216) fused with
+//             C_i V = RHS, blocked by 8 columns (see cta_chol_solve).  The
+//             vectors of node i are
+//               rows of the right slot     -> F = E[o_l+i/s] C_i^{-T}   (K3 trsm_rltn, :219-248)
+//               columns of the left slot   -> G = C_i^{-1} E[o_l+(i-s)/s] (K4 trsm_llnn, :251-279)
+//               columns of y_i (factor_and_solve) -> y_i <- C_i^{-1} y_i (:108-110)
 //   k_update  one CTA per 32x32 output tile:
 //             target j = 2 s u - 1 (owner computes; the reference uses
 //             atomics here, K5/K6 :282-342)
 //                 L_j -= F_{j-s} F_{j-s}^T + G_{j+s}^T G_{j+s}
 //             fill-in for nodes with both neighbours (K7, :345-377)
 //                 E[o_{l+1} + t - 1] -= F_t G_t
-// Substitution sweeps (K9-K16, :425-736):
-//   k_fwd_node     y_i <- C_i^{-1} y_i           (levels ascending)
-//   k_fwd_update   y_j -= F_{j-s} y_{j-s} + G_{j+s}^T y_{j+s}   (owner computes)
-//   k_bwd          x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
-//                  (levels descending)
+// Substitution sweeps (K9-K16, :425-736), reading only lower(L_i):
+//   k_fwd          levels ascending, one launch per level: each vector pulls
+//                  the previous level's coupling updates
+//                  y_j -= F_{j-s/2} y_{j-s/2} + G_{j+s/2}^T y_{j+s/2} and the
+//                  level's nodes then solve y_i <- C_i^{-1} y_i
+//   k_bwd          levels descending: x_i -= F_i^T x_{i+s} + G_i x_{i-s};
+//                  x_i <- C_i^{-T} x_i
 #pragma once
 
 #include "nd_device.cuh"
 
 namespace socu {
 
-constexpr int kDiagBS = 16;   // diagonal block of the in-CTA blocked Cholesky
-constexpr int kTile = 32;     // output tile / panel width
-constexpr int kMC = 32;       // RHS columns handled per pass
+constexpr int kTile = 32;     // output tile / streamed chunk width
+constexpr int kMC = 32;       // RHS columns handled per pass in the sweeps
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ inline int min_i(int a, int b) { return a < b ? a : b; }
 
 // shared-memory sizes (elements) ------------------------------------------------
-__host__ __device__ inline int diag_ld(int n) { return n + 1; }
-__host__ __device__ inline long long smem_diag_elems(int n, int m) {
-  const int mc = m < kMC ? m : kMC;
-  return (long long)n * diag_ld(n) + n + (long long)n * kDiagBS + (long long)n * (mc > 0 ? mc : 0);
+__host__ __device__ inline int gemm_ld(int n, int es) { return es == 8 ? ((n + 15) / 16) * 16 + 4 : n + 1; }
+// vectors solved per pass of k_node: one thread per panel row or vector
+__host__ __device__ inline int node_chunk(int n) { return n <= 64 ? 256 - n : 64; }
+__host__ __device__ inline long long smem_node_elems(int n, int es) {
+  return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n), es);
 }
-__host__ __device__ inline long long smem_couple_elems(int n) {
-  return (long long)n * diag_ld(n) + (long long)n * (kTile + 1);
-}
-__host__ __device__ inline long long smem_update_elems(int n) {
-  return 2LL * kTile * (n + 1) + 2LL * n * (kTile + 1);
+__host__ __device__ inline int update_ld(int k, int es) { return gemm_ld(k, es); }
+__host__ __device__ inline long long smem_update_elems(int n, int es) {
+  const long long a = 2LL * kTile * update_ld(2 * n, es);
+  const long long f = (long long)kTile * update_ld(n, es) + (long long)n * update_ld(kTile, es);
+  return a > f ? a : f;
 }
 __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
-  const int mc = m < kMC ? m : kMC;
-  return 3LL * n * mc + (long long)n * (kTile + 1) + kTile;
+  const int mc = min_i(m, kMC);
+  return 3LL * n * (mc + 1) + (long long)n * (kTile + 1) + kTile;
 }
 
 // ---------------------------------------------------------------------------
-// k_diag
+// k_node: 256 threads per level node i.
+//   C_i = chol(L_i)  (potrf, K2)  fused with  C_i V = RHS for the node's
+//   vectors: rows of the right slot (-> F), columns of the left slot (-> G)
+//   and, with WITH_Y, the columns of y_i, in passes of node_chunk(n) vectors
+//   (the first pass factors, later passes reuse the factor).
 // ---------------------------------------------------------------------------
 template <typename T, bool WITH_Y>
-__global__ void __launch_bounds__(256) k_diag(Problem<T> p, Level lv) {
+__global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
+  constexpr int es = sizeof(T);
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
   if (!p.active(b)) return;
-  const int n = p.n, ld = diag_ld(n);
-  const int i = lv.s - 1 + 2 * lv.s * t;
+  const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
+  const bool right = i + s < p.N, left = t >= 1;
+  const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0;
+  const int NV = nr + nl + ny;
+  const int vc = node_chunk(n), lda = gemm_ld(n, es), ldv = gemm_ld(vc, es);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* A = reinterpret_cast<T*>(smem_raw);
-  T* dinv = A + n * ld;
-  T* P = dinv + n;
-  T* Y = P + n * kDiagBS;
+  T* V = A + n * lda;
 
   T* Li = p.Lb(b, i);
-  load_block(A, ld, Li, n, n, n);
-  __syncthreads();
-  cta_chol_inv<T, kDiagBS>(A, ld, n, dinv, P);
-  store_block(Li, n, A, ld, n, n);
+  T* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
+  T* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
+  T* yi = WITH_Y ? p.Xb(b, i) : nullptr;
 
-  if (WITH_Y) {
-    T* yi = p.Xb(b, i);
-    for (int c0 = 0; c0 < p.m; c0 += kMC) {
-      const int mc = min(kMC, p.m - c0);
-      __syncthreads();
-      load_block(Y, mc, yi + c0, n, mc, p.m);
-      __syncthreads();
-      // y_i <- W y_i with W = C^{-1}: W[r][k] = A[k*ld + r] (k<r), dinv[r] on the diagonal
-      cta_gemm<T, 2, 2, false>(
-          n, mc, n,
-          [&](int r, int k) { return k < r ? A[k * ld + r] : (k == r ? dinv[r] : T(0)); },
-          [&](int k, int c) { return Y[k * mc + c]; },
-          [&](int r, int c, T v) { yi[(long long)r * p.m + c0 + c] = v; });
+  // chunk [v0, v1) of the node's vectors: R rows, then Lf columns, then y columns
+  auto chunk_io = [&](int v0, bool load) {
+    const int v1 = min_i(NV, v0 + vc);
+    const int rA = v0, rB = min_i(v1, nr);
+    const int lS = max(v0, nr), lA = lS - nr, lB = min_i(v1, nr + nl) - nr;
+    const int yS = max(v0, nr + nl), yA = yS - nr - nl, yB = v1 - nr - nl;
+    if (load) {
+      if (rB > rA) async_load_t(V, ldv, R + (long long)rA * n, rB - rA, n, n);
+      if (lB > lA) async_load(V + (lS - v0), ldv, Lf + lA, n, lB - lA, n);
+      if (yB > yA) async_load(V + (yS - v0), ldv, yi + yA, n, yB - yA, p.m);
+    } else {
+      if (rB > rA) store_block_t(R + (long long)rA * n, n, V, ldv, rB - rA, n);
+      if (lB > lA) store_block(Lf + lA, n, V + (lS - v0), ldv, n, lB - lA);
+      if (yB > yA) store_block(yi + yA, p.m, V + (yS - v0), ldv, n, yB - yA);
     }
-  }
-}
+  };
 
-// ---------------------------------------------------------------------------
-// k_couple
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) k_couple(Problem<T> p, Level lv) {
-  const int n = p.n, ld = diag_ld(n);
-  const int np = ceil_div(n, kTile);
-  const int per_b = lv.d * 2 * np;
-  const int b = blockIdx.x / per_b;
-  int rem = blockIdx.x - b * per_b;
-  const int t = rem / (2 * np);
-  rem -= t * 2 * np;
-  const int side = rem / np;        // 0 right, 1 left
-  const int pnl = rem - side * np;
-  if (!p.active(b)) return;
-  const int i = lv.s - 1 + 2 * lv.s * t;
-  if (side == 0 && i + lv.s >= p.N) return;
-  if (side == 1 && t == 0) return;
-  const int p0 = pnl * kTile, pw = min(kTile, n - p0);
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Wt = reinterpret_cast<T*>(smem_raw);   // n x ld, upper triangular = C^{-T}
-  T* Pn = Wt + n * ld;                       // panel
-
-  const T* Li = p.Lb(b, i);
+  async_load(A, lda, Li, n, n, n);
+  if (NV > 0) chunk_io(0, true);
+  cp_async_wait_all();
+  __syncthreads();
+  cta_chol_solve<T, true>(A, lda, n, V, ldv, min_i(NV, vc));
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
-    const T v = Li[e];
-    Wt[r * ld + c] = r < c ? v : (r == c ? rcp_t(v) : T(0));
+    Li[e] = c <= r ? A[r * lda + c] : T(0);
   }
-  if (side == 0) {
-    T* R = p.Eb(b, lv.oc + 2 * t);
-    // rows [p0, p0+pw) of R, all n columns
-    load_block(Pn, ld, R + (long long)p0 * n, pw, n, n);
+  if (NV > 0) chunk_io(0, false);
+  for (int v0 = vc; v0 < NV; v0 += vc) {
     __syncthreads();
-    // F[p0+r][c] = sum_{k<=c} R[p0+r][k] Wt[k][c]
-    cta_gemm<T, 2, 2, false>(
-        pw, n, n,
-        [&](int r, int k) { return Pn[r * ld + k]; },
-        [&](int k, int c) { return Wt[k * ld + c]; },
-        [&](int r, int c, T v) { R[(long long)(p0 + r) * n + c] = v; });
-  } else {
-    T* Gs = p.Eb(b, lv.oc + 2 * t - 1);
-    // columns [p0, p0+pw) of the slot, all n rows; stored as n x (kTile+1)
-    load_block(Pn, kTile + 1, Gs + p0, n, pw, n);
+    chunk_io(v0, true);
+    cp_async_wait_all();
     __syncthreads();
-    // G[r][p0+c] = sum_{k<=r} Wt[k][r] Lf[k][p0+c]
-    cta_gemm<T, 2, 2, false>(
-        n, pw, n,
-        [&](int r, int k) { return Wt[k * ld + r]; },
-        [&](int k, int c) { return Pn[k * (kTile + 1) + c]; },
-        [&](int r, int c, T v) { Gs[(long long)r * n + p0 + c] = v; });
+    cta_chol_solve<T, false>(A, lda, n, V, ldv, min_i(NV - v0, vc));
+    chunk_io(v0, false);
   }
 }
 
@@ -155,6 +128,7 @@ __device__ __forceinline__ void lower_tile_index(int lt, int& ta, int& tc) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
+  constexpr int es = sizeof(T);
   const int n = p.n, N = p.N, s = lv.s;
   const int nt = ceil_div(n, kTile);
   const int nlt = nt * (nt + 1) / 2;
@@ -166,12 +140,7 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
   if (!p.active(b)) return;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* S0 = reinterpret_cast<T*>(smem_raw);
-  const int ldr = n + 1;               // row panels: kTile x (n+1)
-  T* Fa = S0;
-  T* Fc = Fa + kTile * ldr;
-  T* Ga = Fc + kTile * ldr;            // column panels: n x (kTile+1)
-  T* Gc = Ga + n * (kTile + 1);
+  T* Ab = reinterpret_cast<T*>(smem_raw);
 
   if (task < U * nlt) {
     const int u = task / nlt + 1;
@@ -181,24 +150,28 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
     const T* F = p.Eb(b, lv.oc + 2 * (u - 1));
     const bool hasG = j + s < N;
     const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
-    const int ra = ta * kTile, wa = min(kTile, n - ra);
-    const int rc = tc * kTile, wc = min(kTile, n - rc);
-    load_block(Fa, ldr, F + (long long)ra * n, wa, n, n);
-    load_block(Fc, ldr, F + (long long)rc * n, wc, n, n);
-    if (hasG) {
-      load_block(Ga, kTile + 1, G + ra, n, wa, n);
-      load_block(Gc, kTile + 1, G + rc, n, wc, n);
+    const int r0 = ta * kTile, wa = min_i(kTile, n - r0);
+    const int c0 = tc * kTile, wc = min_i(kTile, n - c0);
+    const bool diag = ta == tc;
+    const int K = hasG ? 2 * n : n;
+    const int lda = update_ld(K, es);       // rows of [F | G^T]
+    T* Bb = Ab + kTile * lda;
+    T* Bop = diag ? Ab : Bb;
+    // Ab[r][k] = F[r0+r][k], Ab[r][n+k] = G[k][r0+r]   (k < n)
+    async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);
+    if (hasG) async_load_t(Ab + n, lda, G + r0, n, wa, n);
+    if (!diag) {
+      async_load(Bb, lda, F + (long long)c0 * n, wc, n, n);
+      if (hasG) async_load_t(Bb + n, lda, G + c0, n, wc, n);
     }
+    cp_async_wait_all();
     __syncthreads();
     T* Lj = p.Lb(b, j);
-    const int K = hasG ? 2 * n : n;
-    auto body = [&](int r, int c, T v) { Lj[(long long)(ra + r) * n + rc + c] -= v; };
-    auto fa = [&](int r, int k) { return k < n ? Fa[r * ldr + k] : Ga[(k - n) * (kTile + 1) + r]; };
-    auto fb = [&](int k, int c) { return k < n ? Fc[c * ldr + k] : Gc[(k - n) * (kTile + 1) + c]; };
-    if (ta == tc)
-      cta_gemm<T, 2, 2, true>(wa, wc, K, fa, fb, body);
+    auto out = [&](int r, int c, T v) { Lj[(long long)(r0 + r) * n + c0 + c] -= v; };
+    if (diag)
+      cta_gemm<T, false, true, true>(wa, wc, K, Ab, lda, Bop, lda, out);
     else
-      cta_gemm<T, 2, 2, false>(wa, wc, K, fa, fb, body);
+      cta_gemm<T, false, true, false>(wa, wc, K, Ab, lda, Bop, lda, out);
   } else {
     const int f = task - U * nlt;
     const int t = f / (nt * nt) + 1;
@@ -209,77 +182,74 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
     const T* F = p.Eb(b, lv.oc + 2 * t);
     const T* G = p.Eb(b, lv.oc + 2 * t - 1);
     T* X = p.Eb(b, lv.on + t - 1);
-    const int ra = ta * kTile, wa = min(kTile, n - ra);
-    const int rc = tc * kTile, wc = min(kTile, n - rc);
-    load_block(Fa, ldr, F + (long long)ra * n, wa, n, n);
-    load_block(Ga, kTile + 1, G + rc, n, wc, n);
+    const int r0 = ta * kTile, wa = min_i(kTile, n - r0);
+    const int c0 = tc * kTile, wc = min_i(kTile, n - c0);
+    const int lda = update_ld(n, es), ldg = update_ld(kTile, es);
+    T* Bb = Ab + kTile * lda;
+    async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);   // F rows
+    async_load(Bb, ldg, G + c0, n, wc, n);                    // G columns, n x wc
+    cp_async_wait_all();
     __syncthreads();
-    cta_gemm<T, 2, 2, false>(
-        wa, wc, n,
-        [&](int r, int k) { return Fa[r * ldr + k]; },
-        [&](int k, int c) { return Ga[k * (kTile + 1) + c]; },
-        [&](int r, int c, T v) { X[(long long)(ra + r) * n + rc + c] -= v; });
+    cta_gemm<T, false, false>(wa, wc, n, Ab, lda, Bb, ldg,
+                              [&](int r, int c, T v) { X[(long long)(r0 + r) * n + c0 + c] -= v; });
   }
 }
 
 // ---------------------------------------------------------------------------
-// Sweeps.  Shared layout: Y, Z1, Z2 (n x mc each), Cc (n x (kTile+1)), dv (kTile)
+// Sweeps.  Shared layout: Y, Z1, Z2 (n x (mc+1) each), Cc (n x (kTile+1)), dv (kTile)
 // ---------------------------------------------------------------------------
 
 // Y -= op(M) Z with M an n x n global block, streamed through Cc in kTile
 // chunks of the contraction index.  TRANS: out[r][c] = sum_k M[k][r] Z[k][c].
 template <typename T, bool TRANS>
-__device__ void sweep_accumulate(T* Y, const T* Z, int mc, const T* __restrict__ M, int n, T* Cc) {
+__device__ void sweep_accumulate(T* Y, const T* Z, int ldy, int mc, const T* __restrict__ M, int n, T* Cc) {
+  constexpr int ldc = kTile + 1;
   for (int k0 = 0; k0 < n; k0 += kTile) {
-    const int kw = min(kTile, n - k0);
+    const int kw = min_i(kTile, n - k0);
     __syncthreads();
-    if (TRANS) {
-      // rows [k0, k0+kw) of M, stored transposed: Cc[r * (kTile+1) + kk] = M[k0+kk][r]
-      for (int e = threadIdx.x; e < kw * n; e += blockDim.x) {
-        const int kk = e / n, r = e - kk * n;
-        Cc[r * (kTile + 1) + kk] = M[(long long)(k0 + kk) * n + r];
-      }
-    } else {
-      // columns [k0, k0+kw) of M: Cc[r * (kTile+1) + kk] = M[r][k0+kk]
-      load_block(Cc, kTile + 1, M + k0, n, kw, n);
-    }
+    if (TRANS)
+      async_load_t(Cc, ldc, M + (long long)k0 * n, kw, n, n);   // Cc[r][kk] = M[k0+kk][r]
+    else
+      async_load(Cc, ldc, M + k0, n, kw, n);                   // Cc[r][kk] = M[r][k0+kk]
+    cp_async_wait_all();
     __syncthreads();
-    cta_gemm<T, 2, 1, false>(
-        n, mc, kw,
-        [&](int r, int k) { return Cc[r * (kTile + 1) + k]; },
-        [&](int k, int c) { return Z[(k0 + k) * mc + c]; },
-        [&](int r, int c, T v) { Y[r * mc + c] -= v; });
+    smem_gemm<T, 2, 1, false, false>(n, mc, kw, Cc, ldc, Z + k0 * ldy, ldy,
+                                     [&](int r, int c, T v) { Y[r * ldy + c] -= v; });
   }
   __syncthreads();
 }
 
 // Y <- C^{-1} Y (lower C = lower(Lb)), blocked by kTile rows, warp per column.
 template <typename T>
-__device__ void sweep_lower_solve(T* Y, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
+__device__ void sweep_lower_solve(T* Y, int ldy, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ldc = n + 1;  // Cc holds n*(kTile+1) >= kb*(n+1) elements
   for (int K = 0; K < n; K += kTile) {
-    const int kb = min(kTile, n - K);
+    const int kb = min_i(kTile, n - K);
     __syncthreads();
-    // rows [K, K+kb), columns [0, K+kb): Cc[r * (n+1) + c]; reuse Cc with row stride n+1
-    // Cc holds n*(kTile+1) >= kb*(n+1) elements.
-    const int ldc = n + 1;
-    for (int e = threadIdx.x; e < kb * (K + kb); e += blockDim.x) {
-      const int r = e / (K + kb), c = e - r * (K + kb);
-      Cc[r * ldc + c] = Lb[(long long)(K + r) * n + c];
-    }
+    async_load(Cc, ldc, Lb + (long long)K * n, kb, K + kb, n);   // rows [K,K+kb), cols [0,K+kb)
+    cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x < kb) dv[threadIdx.x] = rcp_t(Cc[threadIdx.x * ldc + K + threadIdx.x]);
+    if (threadIdx.x < kb) dv[threadIdx.x] = T(1) / Cc[threadIdx.x * ldc + K + threadIdx.x];
     __syncthreads();
     for (int c = warp; c < mc; c += nw) {
-      T v = lane < kb ? Y[(K + lane) * mc + c] : T(0);
-      if (lane < kb)
-        for (int k = 0; k < K; ++k) v = fma(-Cc[lane * ldc + k], Y[k * mc + c], v);
+      T v = lane < kb ? Y[(K + lane) * ldy + c] : T(0);
+      if (lane < kb) {
+        T v2 = T(0);
+        int k = 0;
+        for (; k + 1 < K; k += 2) {
+          v = fma(-Cc[lane * ldc + k], Y[k * ldy + c], v);
+          v2 = fma(-Cc[lane * ldc + k + 1], Y[(k + 1) * ldy + c], v2);
+        }
+        if (k < K) v = fma(-Cc[lane * ldc + k], Y[k * ldy + c], v);
+        v += v2;
+      }
       for (int j = 0; j < kb; ++j) {
-        const T yj = __shfl_sync(0xffffffffu, v, j) * dv[j];
+        const T yj = __shfl_sync(kFull, v, j) * dv[j];
         if (lane == j) v = yj;
         else if (lane > j && lane < kb) v = fma(-Cc[lane * ldc + K + j], yj, v);
       }
-      if (lane < kb) Y[(K + lane) * mc + c] = v;
+      if (lane < kb) Y[(K + lane) * ldy + c] = v;
     }
   }
   __syncthreads();
@@ -287,85 +257,214 @@ __device__ void sweep_lower_solve(T* Y, int mc, const T* __restrict__ Lb, int n,
 
 // Y <- C^{-T} Y (lower C = lower(Lb)), blocks from the bottom, warp per column.
 template <typename T>
-__device__ void sweep_upper_solve(T* Y, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
+__device__ void sweep_upper_solve(T* Y, int ldy, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  constexpr int ldc = kTile + 1;
   const int last = ((n - 1) / kTile) * kTile;
   for (int K = last; K >= 0; K -= kTile) {
-    const int kb = min(kTile, n - K);
+    const int kb = min_i(kTile, n - K);
     __syncthreads();
-    // column panel: rows [K, n), columns [K, K+kb): Cc[(k-K) * (kTile+1) + r] = C[k][K+r]
-    load_block(Cc, kTile + 1, Lb + (long long)K * n + K, n - K, kb, n);
+    // column panel: rows [K, n), columns [K, K+kb): Cc[(k-K)][r] = C[k][K+r]
+    async_load(Cc, ldc, Lb + (long long)K * n + K, n - K, kb, n);
+    cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x < kb) dv[threadIdx.x] = rcp_t(Cc[threadIdx.x * (kTile + 1) + threadIdx.x]);
+    if (threadIdx.x < kb) dv[threadIdx.x] = T(1) / Cc[threadIdx.x * ldc + threadIdx.x];
     __syncthreads();
     for (int c = warp; c < mc; c += nw) {
-      T v = lane < kb ? Y[(K + lane) * mc + c] : T(0);
-      if (lane < kb)
-        for (int k = K + kb; k < n; ++k) v = fma(-Cc[(k - K) * (kTile + 1) + lane], Y[k * mc + c], v);
-      for (int j = kb - 1; j >= 0; --j) {
-        const T xj = __shfl_sync(0xffffffffu, v, j) * dv[j];
-        if (lane == j) v = xj;
-        else if (lane < j) v = fma(-Cc[j * (kTile + 1) + lane], xj, v);
+      T v = lane < kb ? Y[(K + lane) * ldy + c] : T(0);
+      if (lane < kb) {
+        T v2 = T(0);
+        int k = K + kb;
+        for (; k + 1 < n; k += 2) {
+          v = fma(-Cc[(k - K) * ldc + lane], Y[k * ldy + c], v);
+          v2 = fma(-Cc[(k + 1 - K) * ldc + lane], Y[(k + 1) * ldy + c], v2);
+        }
+        if (k < n) v = fma(-Cc[(k - K) * ldc + lane], Y[k * ldy + c], v);
+        v += v2;
       }
-      if (lane < kb) Y[(K + lane) * mc + c] = v;
+      for (int j = kb - 1; j >= 0; --j) {
+        const T xj = __shfl_sync(kFull, v, j) * dv[j];
+        if (lane == j) v = xj;
+        else if (lane < j) v = fma(-Cc[j * ldc + lane], xj, v);
+      }
+      if (lane < kb) Y[(K + lane) * ldy + c] = v;
     }
   }
   __syncthreads();
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_node(Problem<T> p, Level lv) {
-  const int b = blockIdx.x / lv.d;
-  const int t = blockIdx.x - b * lv.d;
-  if (!p.active(b)) return;
-  const int n = p.n, i = lv.s - 1 + 2 * lv.s * t;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int mcmax = min(p.m, kMC);
-  T* Y = reinterpret_cast<T*>(smem_raw);
-  T* Cc = Y + 3 * n * mcmax;
-  T* dv = Cc + n * (kTile + 1);
-  T* yi = p.Xb(b, i);
-  const T* Li = p.Lb(b, i);
-  for (int c0 = 0; c0 < p.m; c0 += kMC) {
-    const int mc = min(kMC, p.m - c0);
-    __syncthreads();
-    load_block(Y, mc, yi + c0, n, mc, p.m);
-    sweep_lower_solve(Y, mc, Li, n, Cc, dv);
-    store_block(yi + c0, p.m, Y, mc, n, mc);
+// ---------------------------------------------------------------------------
+// Resident sweep helpers: the whole factor block and both coupling blocks of
+// a node sit in shared memory (one load round), Y/Z are n x mc column chunks.
+// Leading dimensions are even so every load can be vectorised.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline long long smem_sweep_res_elems(int n, int m) {
+  const int mc = min_i(m, kMC);
+  return 3LL * n * even_ld(n) + 3LL * n * even_ld(mc) + n;
+}
+
+// Y -= op(M) Z, M resident (ld ldm).  TRANS: out[r][c] = sum_k M[k][r] Z[k][c].
+// One thread per output, four independent partial sums.
+template <typename T, bool TRANS>
+__device__ __forceinline__ void res_accumulate(T* Y, const T* Z, int ldy, int mc, const T* M, int ldm, int n) {
+  for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
+    const int r = o / mc, c = o - r * mc;
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
+    int k = 0;
+    for (; k + 3 < n; k += 4) {
+      const T m0 = TRANS ? M[k * ldm + r] : M[r * ldm + k];
+      const T m1 = TRANS ? M[(k + 1) * ldm + r] : M[r * ldm + k + 1];
+      const T m2 = TRANS ? M[(k + 2) * ldm + r] : M[r * ldm + k + 2];
+      const T m3 = TRANS ? M[(k + 3) * ldm + r] : M[r * ldm + k + 3];
+      s0 = fma(m0, Z[k * ldy + c], s0);
+      s1 = fma(m1, Z[(k + 1) * ldy + c], s1);
+      s2 = fma(m2, Z[(k + 2) * ldy + c], s2);
+      s3 = fma(m3, Z[(k + 3) * ldy + c], s3);
+    }
+    for (; k < n; ++k) s0 = fma(TRANS ? M[k * ldm + r] : M[r * ldm + k], Z[k * ldy + c], s0);
+    Y[r * ldy + c] -= (s0 + s1) + (s2 + s3);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_update(Problem<T> p, Level lv) {
-  const int s = lv.s, N = p.N;
-  const int U = N / (2 * s);
-  const int b = blockIdx.x / U;
-  const int u = blockIdx.x - b * U + 1;
+// Y <- C^{-1} Y (UPPER: Y <- C^{-T} Y), C = lower(Cs) resident, dv[r] = 1/C[r][r].
+// Right-looking by 8-row blocks: one thread per column solves the block
+// against the 8x8 diagonal block held in registers, then every (row, column)
+// of the remaining rows takes an 8-term update.
+template <typename T, bool UPPER>
+__device__ void res_tri_solve(T* Y, int ldy, int mc, const T* Cs, int ldc, const T* dv, int n) {
+  constexpr int BK = 8;
+  const int nblk = (n + BK - 1) / BK;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int K = UPPER ? (nblk - 1 - bi) * BK : bi * BK;
+    const int kb = min_i(BK, n - K);
+    for (int c = threadIdx.x; c < mc; c += blockDim.x) {
+      T x[BK];
+#pragma unroll
+      for (int j = 0; j < BK; ++j) x[j] = j < kb ? Y[(K + j) * ldy + c] : T(0);
+      if (!UPPER) {
+#pragma unroll
+        for (int j = 0; j < BK; ++j) {
+          if (j < kb) {
+#pragma unroll
+            for (int i = 0; i < j; ++i) x[j] = fma(-Cs[(K + j) * ldc + K + i], x[i], x[j]);
+            x[j] *= dv[K + j];
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = BK - 1; j >= 0; --j) {
+          if (j < kb) {
+#pragma unroll
+            for (int i = j + 1; i < BK; ++i)
+              if (i < kb) x[j] = fma(-Cs[(K + i) * ldc + K + j], x[i], x[j]);
+            x[j] *= dv[K + j];
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < BK; ++j)
+        if (j < kb) Y[(K + j) * ldy + c] = x[j];
+    }
+    __syncthreads();
+    // remaining rows: below the block (forward) or above it (backward)
+    const int r0 = UPPER ? 0 : K + kb;
+    const int nr = UPPER ? K : n - K - kb;
+    for (int o = threadIdx.x; o < nr * mc; o += blockDim.x) {
+      const int r = r0 + o / mc, c = o - (o / mc) * mc;
+      T acc = T(0);
+#pragma unroll
+      for (int j = 0; j < BK; ++j)
+        if (j < kb) acc = fma(UPPER ? Cs[(K + j) * ldc + r] : Cs[r * ldc + K + j], Y[(K + j) * ldy + c], acc);
+      Y[r * ldy + c] -= acc;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_fwd (level l): pull the level-(l-1) coupling updates and solve.
+//   l == 0: task t -> node i = 2t:  y_i <- C_i^{-1} y_i
+//   l >= 1: task u-1, target j = s*u - 1 of the level-(l-1) updates:
+//           y_j -= F y_{j-s/2} + G^T y_{j+s/2}   (slots o_{l-1}+2u-2, +2u-1)
+//           and for odd u (j is a level-l node) y_j <- C_j^{-1} y_j.
+// Every vector has one writer per launch (K launches per forward sweep).
+// RES: factor and coupling blocks resident in shared memory.
+// ---------------------------------------------------------------------------
+// PULL_ONLY (fused factor_and_solve): apply the updates, never solve.
+template <typename T, bool RES, bool PULL_ONLY = false>
+__global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
+  const int s = lv.s, N = p.N, n = p.n;
+  const int per_b = s == 1 ? lv.d : N / s;
+  const int b = blockIdx.x / per_b;
+  const int task = blockIdx.x - b * per_b;
   if (!p.active(b)) return;
-  const int n = p.n, j = 2 * s * u - 1;
+  const int h = s / 2;
+  int j;
+  bool pull, solve;
+  const T *F = nullptr, *G = nullptr;
+  if (s == 1) {
+    j = 2 * task;
+    pull = false;
+    solve = true;
+  } else {
+    const int u = task + 1;
+    j = s * u - 1;
+    pull = true;
+    solve = !PULL_ONLY && (u & 1) != 0;
+    F = p.Eb(b, lv.op + 2 * u - 2);
+    if (j + h < N) G = p.Eb(b, lv.op + 2 * u - 1);
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int mcmax = min(p.m, kMC);
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
-  T* Z1 = Y + n * mcmax;
-  T* Z2 = Z1 + n * mcmax;
-  T* Cc = Z2 + n * mcmax;
-  const T* F = p.Eb(b, lv.oc + 2 * (u - 1));
-  const bool hasG = j + s < N;
-  const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
+  T* Z1 = Y + n * ldy;
+  T* Z2 = Z1 + n * ldy;
+  T* Ms = Z2 + n * ldy;   // RES: C, F, G (n x ldm each), dv (n); else Cc (n x (kTile+1)), dv
+  const int ldm = even_ld(n);
+  T* Cs = Ms;
+  T* Fs = Cs + n * ldm;
+  T* Gs = Fs + n * ldm;
+  T* dv = RES ? Gs + n * ldm : Ms + n * (kTile + 1);
   T* yj = p.Xb(b, j);
+  const T* Lj = p.Lb(b, j);
+  if (RES) {
+    if (solve) async_load(Cs, ldm, Lj, n, n, n);
+    if (F) async_load(Fs, ldm, F, n, n, n);
+    if (G) async_load(Gs, ldm, G, n, n, n);
+  }
   for (int c0 = 0; c0 < p.m; c0 += kMC) {
-    const int mc = min(kMC, p.m - c0);
+    const int mc = min_i(kMC, p.m - c0);
     __syncthreads();
-    load_block(Y, mc, yj + c0, n, mc, p.m);
-    load_block(Z1, mc, p.Xb(b, j - s) + c0, n, mc, p.m);
-    if (hasG) load_block(Z2, mc, p.Xb(b, j + s) + c0, n, mc, p.m);
-    sweep_accumulate<T, false>(Y, Z1, mc, F, n, Cc);   // Y -= F y_{j-s}
-    if (hasG) sweep_accumulate<T, true>(Y, Z2, mc, G, n, Cc);  // Y -= G^T y_{j+s}
-    store_block(yj + c0, p.m, Y, mc, n, mc);
+    async_load(Y, ldy, yj + c0, n, mc, p.m);
+    if (pull) async_load(Z1, ldy, p.Xb(b, j - h) + c0, n, mc, p.m);
+    if (G) async_load(Z2, ldy, p.Xb(b, j + h) + c0, n, mc, p.m);
+    cp_async_wait_all();
+    __syncthreads();
+    if (RES) {
+      if (c0 == 0 && solve)
+        for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
+      if (pull) {
+        res_accumulate<T, false>(Y, Z1, ldy, mc, Fs, ldm, n);          // Y -= F y_{j-h}
+        __syncthreads();
+        if (G) res_accumulate<T, true>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G^T y_{j+h}
+      }
+      __syncthreads();
+      if (solve) res_tri_solve<T, false>(Y, ldy, mc, Cs, ldm, dv, n);
+    } else {
+      if (pull) {
+        sweep_accumulate<T, false>(Y, Z1, ldy, mc, F, n, Ms);
+        if (G) sweep_accumulate<T, true>(Y, Z2, ldy, mc, G, n, Ms);
+      }
+      if (solve) sweep_lower_solve(Y, ldy, mc, Lj, n, Ms, dv);
+    }
+    store_block(yj + c0, p.m, Y, ldy, n, mc);
   }
 }
 
-template <typename T>
+// ---------------------------------------------------------------------------
+// k_bwd (level l, descending): x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
+// ---------------------------------------------------------------------------
+template <typename T, bool RES>
 __global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
@@ -373,26 +472,48 @@ __global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
   const int n = p.n, s = lv.s, N = p.N;
   const int i = s - 1 + 2 * s * t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int mcmax = min(p.m, kMC);
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
-  T* Z1 = Y + n * mcmax;
-  T* Z2 = Z1 + n * mcmax;
-  T* Cc = Z2 + n * mcmax;
-  T* dv = Cc + n * (kTile + 1);
+  T* Z1 = Y + n * ldy;
+  T* Z2 = Z1 + n * ldy;
+  T* Ms = Z2 + n * ldy;
+  const int ldm = even_ld(n);
+  T* Cs = Ms;
+  T* Fs = Cs + n * ldm;
+  T* Gs = Fs + n * ldm;
+  T* dv = RES ? Gs + n * ldm : Ms + n * (kTile + 1);
   const bool right = i + s < N, left = i >= s;
   const T* F = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
   const T* G = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
+  const T* Li = p.Lb(b, i);
   T* xi = p.Xb(b, i);
+  if (RES) {
+    async_load(Cs, ldm, Li, n, n, n);
+    if (right) async_load(Fs, ldm, F, n, n, n);
+    if (left) async_load(Gs, ldm, G, n, n, n);
+  }
   for (int c0 = 0; c0 < p.m; c0 += kMC) {
-    const int mc = min(kMC, p.m - c0);
+    const int mc = min_i(kMC, p.m - c0);
     __syncthreads();
-    load_block(Y, mc, xi + c0, n, mc, p.m);
-    if (right) load_block(Z1, mc, p.Xb(b, i + s) + c0, n, mc, p.m);
-    if (left) load_block(Z2, mc, p.Xb(b, i - s) + c0, n, mc, p.m);
-    if (right) sweep_accumulate<T, true>(Y, Z1, mc, F, n, Cc);   // Y -= F^T x_{i+s}
-    if (left) sweep_accumulate<T, false>(Y, Z2, mc, G, n, Cc);   // Y -= G x_{i-s}
-    sweep_upper_solve(Y, mc, p.Lb(b, i), n, Cc, dv);
-    store_block(xi + c0, p.m, Y, mc, n, mc);
+    async_load(Y, ldy, xi + c0, n, mc, p.m);
+    if (right) async_load(Z1, ldy, p.Xb(b, i + s) + c0, n, mc, p.m);
+    if (left) async_load(Z2, ldy, p.Xb(b, i - s) + c0, n, mc, p.m);
+    cp_async_wait_all();
+    __syncthreads();
+    if (RES) {
+      if (c0 == 0)
+        for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
+      if (right) res_accumulate<T, true>(Y, Z1, ldy, mc, Fs, ldm, n);    // Y -= F^T x_{i+s}
+      __syncthreads();
+      if (left) res_accumulate<T, false>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G x_{i-s}
+      __syncthreads();
+      res_tri_solve<T, true>(Y, ldy, mc, Cs, ldm, dv, n);
+    } else {
+      if (right) sweep_accumulate<T, true>(Y, Z1, ldy, mc, F, n, Ms);
+      if (left) sweep_accumulate<T, false>(Y, Z2, ldy, mc, G, n, Ms);
+      sweep_upper_solve(Y, ldy, mc, Li, n, Ms, dv);
+    }
+    store_block(xi + c0, p.m, Y, ldy, n, mc);
   }
 }
 

@@ -1,0 +1,258 @@
+// Mixed-precision factorisation with FP64 iterative refinement.
+//
+// The FP64 problem (L, E, b) is left untouched.  A float copy of (L, E) is
+// factored with the same nested-dissection kernels; then
+//     x = 0, r = b
+//     repeat: delta = solve32(r); x += delta; r = b - Psi x (FP64);
+//             eta = ||r||_inf / (||Psi||_inf ||x||_inf + ||b||_inf)
+//     until eta <= tol (per instance) or max_iter
+// Converged instances drop out of every later kernel through the per-instance
+// `active` flags, which the solver kernels take as their batch mask.
+#pragma once
+
+#include "nd_kernels.cuh"
+
+namespace socu {
+
+// Per-instance refinement state, in the caller's workspace.
+struct RefineState {
+  unsigned long long psi;   // ||Psi||_inf bits (non-negative doubles order like uint64)
+  unsigned long long bnorm; // ||b||_inf bits
+  unsigned long long rnorm; // ||r||_inf bits, accumulated per iteration
+  unsigned long long xnorm; // ||x||_inf bits, accumulated per iteration
+};
+
+struct RefineArgs {
+  const double* L;   // (B, N, n, n) original diagonal blocks (lower read)
+  const double* E;   // (B, S, n, n) original off-diagonal storage (slots < N-1 read)
+  const double* b;   // (B, N, n, m)
+  double* x;         // (B, N, n, m) solution
+  const uint8_t* mask;
+  float* L32;
+  float* E32;
+  float* R32;        // (B, N, n, m) residual in / correction out
+  uint8_t* active;
+  RefineState* st;
+  double* eta;       // (B,) last backward error
+  int* iters;        // (B,) iterations performed
+  int* any_active;   // 1 while some instance still iterates
+  double* rout;      // plain residual output (k_residual<false>), else unused
+  int B, N, n, m, S;
+  double tol;
+  int max_iter;
+};
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  }
+  return v;  // valid in thread 0
+}
+
+// Per-instance state reset (before k_ref_init accumulates into it).
+__global__ void k_ref_reset(RefineArgs a) {
+  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
+    const bool on = a.mask == nullptr || a.mask[bi] != 0;
+    a.active[bi] = on ? 1 : 0;
+    a.iters[bi] = 0;
+    a.eta[bi] = on ? __longlong_as_double(0x7ff0000000000000LL) : 0.0;
+    a.st[bi].psi = 0ull;
+    a.st[bi].bnorm = 0ull;
+    a.st[bi].rnorm = 0ull;
+    a.st[bi].xnorm = 0ull;
+    if (on) atomicExch(a.any_active, 1);
+  }
+}
+
+// One CTA per (instance, block index i < max(N, S)): float copies of L_i and
+// slot i, R32 = b, x = 0, ||Psi||_inf and ||b||_inf contributions of block row i.
+__global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
+  const int per = a.N > a.S ? a.N : a.S;
+  const int bi = blockIdx.x / per;
+  const int i = blockIdx.x - bi * per;
+  __shared__ double red[32];
+  const bool on = a.mask == nullptr || a.mask[bi] != 0;
+  const int n = a.n, m = a.m;
+  const long long nn = (long long)n * n;
+  if (!on) return;
+  if (i < a.N) {
+    const double* Li = a.L + ((long long)bi * a.N + i) * nn;
+    float* L32 = a.L32 + ((long long)bi * a.N + i) * nn;
+    for (long long e = threadIdx.x; e < nn; e += blockDim.x) L32[e] = (float)Li[e];
+  }
+  if (i < a.S) {
+    const long long off = ((long long)bi * a.S + i) * nn;
+    float* E32 = a.E32 + off;
+    if (i < a.N - 1) {
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) E32[e] = (float)a.E[off + e];
+    } else {
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) E32[e] = 0.0f;
+    }
+  }
+  if (i >= a.N) return;
+  const long long vo = ((long long)bi * a.N + i) * n * m;
+  double bmax = 0.0;
+  for (int e = threadIdx.x; e < n * m; e += blockDim.x) {
+    const double v = a.b[vo + e];
+    a.R32[vo + e] = (float)v;
+    a.x[vo + e] = 0.0;
+    bmax = fmax(bmax, fabs(v));
+  }
+  // row sums of |Psi| over block row i: lower-symmetric D_i, E_{i-1} rows, E_i columns
+  const double* Li = a.L + ((long long)bi * a.N + i) * nn;
+  const double* Em = i > 0 ? a.E + ((long long)bi * a.S + i - 1) * nn : nullptr;
+  const double* Ei = i < a.N - 1 ? a.E + ((long long)bi * a.S + i) * nn : nullptr;
+  double rmax = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double sum = 0.0;
+    for (int c = 0; c < n; ++c) sum += fabs(c <= r ? Li[(long long)r * n + c] : Li[(long long)c * n + r]);
+    if (Em)
+      for (int c = 0; c < n; ++c) sum += fabs(Em[(long long)r * n + c]);
+    if (Ei)
+      for (int c = 0; c < n; ++c) sum += fabs(Ei[(long long)c * n + r]);
+    rmax = fmax(rmax, sum);
+  }
+  const double bm = block_max(bmax, red);
+  const double pm = block_max(rmax, red);
+  if (threadIdx.x == 0) {
+    atomic_max_pos(&a.st[bi].bnorm, bm);
+    atomic_max_pos(&a.st[bi].psi, pm);
+  }
+}
+
+// x += delta (R32) for active instances; grid-stride over the whole batch.
+__global__ void __launch_bounds__(256) k_ref_update(RefineArgs a) {
+  const long long per = (long long)a.N * a.n * a.m;
+  const long long total = (long long)a.B * per;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int bi = (int)(e / per);
+    if (a.active[bi]) a.x[e] += (double)a.R32[e];
+  }
+}
+
+// r = b - Psi x for rows [r0, r0+32) of block row i (FP64 against the
+// original blocks), R32 = float(r), ||r||_inf and ||x||_inf accumulated.
+// Shared: Lr (32 x ldn) rows of L_i, Lc (n x 33) column panel of L_i,
+// Er (32 x ldn) rows of E_{i-1}, Ec (n x 33) columns of E_i, X (3 x n x ldx).
+constexpr int kResRows = 32;
+constexpr int kResCols = 16;
+__host__ __device__ inline long long smem_residual_elems(int n) {
+  return 2LL * kResRows * (n + 1) + 2LL * n * (kResRows + 1) + 3LL * n * (kResCols + 1);
+}
+
+// REFINE: write R32 = float(r), accumulate norms, skip inactive instances.
+// Otherwise write r (double) to a.rout for every instance.
+template <bool REFINE>
+__global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
+  const int n = a.n, m = a.m, N = a.N;
+  const int nrc = (n + kResRows - 1) / kResRows;
+  const int per = N * nrc;
+  const int bi = blockIdx.x / per;
+  const int rem = blockIdx.x - bi * per;
+  const int i = rem / nrc;
+  const int r0 = (rem - i * nrc) * kResRows;
+  const int rw = min(kResRows, n - r0);
+  if (REFINE && !a.active[bi]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ldn = n + 1, ldc = kResRows + 1, ldx = kResCols + 1;
+  double* Lr = reinterpret_cast<double*>(smem_raw);
+  double* Er = Lr + kResRows * ldn;
+  double* Lc = Er + kResRows * ldn;
+  double* Ec = Lc + n * ldc;
+  double* X0 = Ec + n * ldc;   // x_{i-1}
+  double* X1 = X0 + n * ldx;   // x_i
+  double* X2 = X1 + n * ldx;   // x_{i+1}
+  __shared__ double red[32];
+  const long long nn = (long long)n * n;
+  const double* Li = a.L + ((long long)bi * N + i) * nn;
+  const bool hasm = i > 0, hasp = i < N - 1;
+  const double* Em = hasm ? a.E + ((long long)bi * a.S + i - 1) * nn : nullptr;
+  const double* Ei = hasp ? a.E + ((long long)bi * a.S + i) * nn : nullptr;
+  async_load(Lr, ldn, Li + (long long)r0 * n, rw, n, n);
+  async_load(Lc, ldc, Li + r0, n, rw, n);
+  if (hasm) async_load(Er, ldn, Em + (long long)r0 * n, rw, n, n);
+  if (hasp) async_load(Ec, ldc, Ei + r0, n, rw, n);
+  const long long vi = ((long long)bi * N + i) * n * m;
+  double rmax = 0.0, xmax = 0.0;
+  for (int c0 = 0; c0 < m; c0 += kResCols) {
+    const int mc = min(kResCols, m - c0);
+    __syncthreads();
+    async_load(X1, ldx, a.x + vi + c0, n, mc, m);
+    if (hasm) async_load(X0, ldx, a.x + vi - (long long)n * m + c0, n, mc, m);
+    if (hasp) async_load(X2, ldx, a.x + vi + (long long)n * m + c0, n, mc, m);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int o = threadIdx.x; o < rw * mc; o += blockDim.x) {
+      const int rr = o / mc, c = o - rr * mc, r = r0 + rr;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      // D_i x_i with D symmetric from lower(L_i): k <= r from row r, k > r from column r
+      for (int k = 0; k <= r; ++k) s0 = fma(Lr[rr * ldn + k], X1[k * ldx + c], s0);
+      for (int k = r + 1; k < n; ++k) s0 = fma(Lc[k * ldc + rr], X1[k * ldx + c], s0);
+      if (hasm)
+        for (int k = 0; k < n; ++k) s1 = fma(Er[rr * ldn + k], X0[k * ldx + c], s1);
+      if (hasp)
+        for (int k = 0; k < n; ++k) s2 = fma(Ec[k * ldc + rr], X2[k * ldx + c], s2);
+      const long long e = vi + (long long)r * m + c0 + c;
+      const double res = a.b[e] - (s0 + s1 + s2);
+      if (REFINE) {
+        a.R32[e] = (float)res;
+        const double xv = X1[r * ldx + c];
+        // non-finite values poison the norms (fmax alone would drop a NaN)
+        rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
+        xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
+      } else {
+        a.rout[e] = res;
+      }
+    }
+  }
+  if (REFINE) {
+    const double rm = block_max(rmax, red);
+    const double xm = block_max(xmax, red);
+    if (threadIdx.x == 0) {
+      atomic_max_pos(&a.st[bi].rnorm, rm);
+      atomic_max_pos(&a.st[bi].xnorm, xm);
+    }
+  }
+}
+
+// Convergence test per instance; clears the accumulators for the next round.
+// A non-finite eta (numerical breakdown of the float factor) stops the
+// instance with iters = -(iterations done).
+__global__ void k_ref_check(RefineArgs a) {
+  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
+    if (!a.active[bi]) continue;
+    RefineState& s = a.st[bi];
+    const double rn = __longlong_as_double((long long)s.rnorm);
+    const double xn = __longlong_as_double((long long)s.xnorm);
+    const double pn = __longlong_as_double((long long)s.psi);
+    const double bn = __longlong_as_double((long long)s.bnorm);
+    const double den = pn * xn + bn;
+    const double eta = den > 0.0 ? rn / den : 0.0;
+    const int it = a.iters[bi] + 1;
+    a.iters[bi] = it;
+    a.eta[bi] = eta;
+    s.rnorm = 0ull;
+    s.xnorm = 0ull;
+    if (!(eta == eta) || isinf(eta)) {
+      a.active[bi] = 0;
+      a.iters[bi] = -it;
+    } else if (eta <= a.tol || it >= a.max_iter) {
+      a.active[bi] = 0;
+    } else {
+      atomicExch(a.any_active, 1);
+    }
+  }
+}
+
+}  // namespace socu

@@ -72,11 +72,11 @@ def test_invalid_arguments_rejected_without_gpu(lib):
 
 
 def test_launch_kernel_count_without_gpu(lib):
-    # counting needs no device: per level diag (+couple, update) for the factor
+    # counting needs no device: per level node (+ update) for the factor
     h = ctypes.c_void_p()
     fake = 0x1000  # never dereferenced: counting mode does not launch
     st = lib.socu_launch_create(ctypes.byref(h), _lib.OP_FACTOR, _lib.FLOAT64, fake, fake, None, None,
                                 1, 100, 32, 0, 0, None)
     assert st == 0
-    assert lib.socu_launch_kernel_count(h) == (7 - 1) * 3 + 1  # K = 7 levels, last one diag only
+    assert lib.socu_launch_kernel_count(h) == (7 - 1) * 2 + 1  # K = 7 levels: node + update, last one node only
     lib.socu_launch_destroy(h)
