@@ -33,6 +33,7 @@ extern "C" {
 #define SOCU_ERR_CUDA (-2)
 #define SOCU_ERR_UNSUPPORTED (-3)
 #define SOCU_ERR_TIMEOUT (-4)
+#define SOCU_ERR_SCRATCH_TOO_SMALL (-5)
 
 typedef enum socu_dtype { SOCU_FLOAT32 = 0, SOCU_FLOAT64 = 1 } socu_dtype;
 
@@ -130,6 +131,28 @@ int socu_refine_launch_create(socu_launch_t* out, const double* L, const double*
                               const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                               int max_iter, double tol, void* workspace, size_t workspace_bytes, double* eta,
                               int32_t* iters, int use_cuda_graph, void* stream);
+
+/* Same solve as socu_refine_solve, for callers that cannot allocate device
+ * memory while they solve: an XLA/JAX custom call (buffers come from XLA's
+ * allocator, the handler must not cudaMalloc), a real-time control loop that
+ * bans allocation after start-up (cudaMalloc/cudaFree can block and
+ * synchronise the device), or code running inside CUDA stream capture, where
+ * cudaMalloc is not allowed.  No counterpart in the reference.
+ * Nothing is allocated: the float factor, the correction vector and the
+ * per-instance refinement state live in one fixed array of
+ * SOCU_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads
+ * the library holds until the process exits.  Problems whose scratch
+ * (socu_refine_workspace_bytes) exceeds it are rejected with
+ * SOCU_ERR_SCRATCH_TOO_SMALL.  The first call on each device looks the
+ * array's device address up (make that first call before any stream
+ * capture).  All calls share the one array: every call re-initialises what it
+ * reads, but calls whose work overlaps on the GPU (different streams, or
+ * different host threads on the same device) race and corrupt each other. */
+#define SOCU_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+
+int socu_refine_solve_noalloc(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
+                              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
+                              double* eta, int32_t* iters, void* stream);
 
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */

@@ -20,6 +20,7 @@ STATUS_TEXT = {
     -2: "CUDA error",
     -3: "unsupported problem size",
     -4: "device wait timed out",
+    -5: "problem needs more scratch than the fixed no-allocation array holds",
 }
 
 FLOAT32 = 0
@@ -62,6 +63,8 @@ _SIGNATURES = {
     "socu_refine_launch_create": (_int, [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64,
                                          _int, ctypes.c_double, _vp, ctypes.c_size_t, _vp, _vp, _int, _vp]),
     "socu_block_tridiag_residual": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
+    "socu_refine_solve_noalloc": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,
+                                         _vp, _vp, _vp]),
 }
 
 

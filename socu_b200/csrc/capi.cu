@@ -391,6 +391,113 @@ int capture(socu_launch_s* h) {
 }
 }  // namespace
 
+
+// ---------------------------------------------------------------------------
+// Refined solve without any allocation.
+//
+// Some callers cannot allocate device memory while they solve: an XLA/JAX
+// custom call receives its buffers from XLA's allocator and must not call
+// cudaMalloc inside the handler; a real-time MPC loop forbids allocation
+// after start-up because cudaMalloc/cudaFree can block for an unbounded time
+// and synchronise the device; and cudaMalloc is not allowed while a stream
+// is being captured into a CUDA graph.  For them the float factor, the
+// correction vector and the per-instance refinement state live in the fixed
+// array below instead of a caller workspace.  The host side uses only stack
+// storage.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // == SOCU_NOALLOC_SCRATCH_BYTES
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device (with that device current) and cached.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dev < 0 || dev >= kMaxDevices) return SOCU_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e);
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SOCU_OK;
+}
+
+template <typename K>
+cudaError_t noalloc_smem(K kernel, size_t smem) {
+  return smem > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                          : cudaSuccess;
+}
+
+// Same kernel sequence as refine_enqueue, with the level schedule on the stack.
+int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
+  Level lv[32];
+  int K = 0;
+  for (int s = 1, prev = 0, curr = 0, nxt = a.N - 1; K < (int)socu_recursive_iterations(a.N); ++K) {
+    lv[K].s = s;
+    lv[K].d = (a.N + s) / (2 * s);
+    lv[K].oc = curr;
+    lv[K].on = nxt;
+    lv[K].op = prev;
+    s *= 2;
+    prev = curr;
+    curr = nxt;
+    nxt += a.N / s - 1;
+  }
+  const Dims d{a.B, a.N, a.n, a.m, a.S};
+  const Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
+  const Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
+  const int n = a.n, nth = threads_for(n);
+  const size_t sd = smem_node_elems(n, sizeof(float)) * sizeof(float);
+  const size_t su = smem_update_elems(n, sizeof(float)) * sizeof(float);
+  const bool res = (long long)smem_sweep_res_elems(n, a.m) * (long long)sizeof(float) <= (long long)max_smem_optin();
+  const size_t ss = (res ? smem_sweep_res_elems(n, a.m) : smem_sweep_elems(n, a.m)) * sizeof(float);
+  const size_t sres = smem_residual_elems(n) * sizeof(double);
+  auto fwd = res ? k_fwd<float, true> : k_fwd<float, false>;
+  auto bwd = res ? k_bwd<float, true> : k_bwd<float, false>;
+  cudaError_t e = noalloc_smem(k_node<float, false>, sd);
+  if (e == cudaSuccess) e = noalloc_smem(k_update<float>, su);
+  if (e == cudaSuccess) e = noalloc_smem(fwd, ss);
+  if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
+  if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
+  if (e != cudaSuccess) return cuda_status(e);
+  const int nt = ceil_div(n, kTile), nlt = nt * (nt + 1) / 2;
+  const int nrc = ceil_div(n, kResRows);
+  const long long nvec = (long long)a.B * a.N * a.n * a.m;
+  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
+  const int chk_blocks = (a.B + 255) / 256;
+  e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_status(e);
+  k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
+  k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+  for (int l = 0; l < K; ++l) {
+    k_node<float, false><<<(unsigned)((long long)a.B * lv[l].d), 256, sd, st>>>(pfac, lv[l]);
+    if (l + 1 < K) {
+      const long long blocks = (long long)a.B * ((a.N / (2 * lv[l].s)) * nlt + (lv[l].d - 1) * nt * nt);
+      if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pfac, lv[l]);
+    }
+  }
+  for (int it = 0; it < a.max_iter; ++it) {
+    for (int l = 0; l < K; ++l)
+      fwd<<<(unsigned)((long long)a.B * (l == 0 ? lv[l].d : a.N / lv[l].s)), nth, ss, st>>>(pf, lv[l]);
+    for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
+    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+    k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
+  }
+  return cuda_status(cudaGetLastError());
+}
+}  // namespace
+
 extern "C" {
 
 const char* socu_version(void) { return "socu_b200 0.1.0 (sm_100a)"; }
@@ -402,6 +509,8 @@ const char* socu_status_string(int status) {
     case SOCU_ERR_CUDA: return "CUDA error";
     case SOCU_ERR_UNSUPPORTED: return "unsupported problem size";
     case SOCU_ERR_TIMEOUT: return "device wait timed out";
+    case SOCU_ERR_SCRATCH_TOO_SMALL:
+      return "problem needs more scratch than the fixed no-allocation array holds (SOCU_NOALLOC_SCRATCH_BYTES)";
     default: return "unknown status";
   }
 }
@@ -605,6 +714,29 @@ int socu_launch_destroy(socu_launch_t h) {
   if (h->graph) cudaGraphDestroy(h->graph);
   delete h;
   return SOCU_OK;
+}
+
+
+int socu_refine_solve_noalloc(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
+                              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
+                              double* eta, int32_t* iters, void* stream) {
+  if (batch < 0 || horizon <= 0 || n <= 0 || n_rhs <= 0) return SOCU_ERR_INVALID_ARGUMENT;
+  if (refine_layout(batch, horizon, n, n_rhs).total > kNoAllocScratchBytes) return SOCU_ERR_SCRATCH_TOO_SMALL;
+  Dims d;
+  const int v = validate(SOCU_OP_SOLVE, SOCU_FLOAT32, L, E, x, batch, horizon, n, n_rhs, &d);
+  if (v != SOCU_OK) return v;
+  if (max_iter < 1 || max_iter > 1000 || !(tol >= 0.0)) return SOCU_ERR_INVALID_ARGUMENT;
+  if (batch == 0) return SOCU_OK;
+  if (b == nullptr || eta == nullptr || iters == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  if ((long long)smem_residual_elems(d.n) * (long long)sizeof(double) > (long long)max_smem_optin())
+    return SOCU_ERR_UNSUPPORTED;
+  cudaError_t e = ensure_device(L);
+  if (e != cudaSuccess) return cuda_status(e);
+  void* scratch = nullptr;
+  const int st = noalloc_scratch(&scratch);
+  if (st != SOCU_OK) return st;
+  const RefineArgs a = refine_args(L, E, b, x, mask, d, max_iter, tol, scratch, eta, iters);
+  return refine_enqueue_noalloc(a, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"
