@@ -285,7 +285,7 @@ def run_ours(args, rank, world, local_rank):
                                    f"({[round(t, 3) for t in cpu_ts]} s)"},
         "e2e": {"value": world / sec_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": sec_e2e * 1e3},
-        "gpu_launches": mixed.kernel_count * args.steps,
+        "gpu_launches": (mixed.kernel_count + abs(iters) * mixed.round_kernel_count) * args.steps,
         "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -104,8 +104,13 @@ int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L
 
 int socu_launch_run(socu_launch_t launch, void* stream);
 
-/* Number of kernels one run enqueues (0 for a NULL launch). */
+/* Number of kernels one run enqueues (0 for a NULL launch).  For a
+ * graph-captured refined solve: the kernels before the refinement loop. */
 int64_t socu_launch_kernel_count(socu_launch_t launch);
+
+/* Graph-captured refined solve: kernels per refinement round (the rounds run
+ * in a conditional WHILE node until every instance converged); 0 otherwise. */
+int64_t socu_launch_round_kernel_count(socu_launch_t launch);
 
 int socu_launch_destroy(socu_launch_t launch);
 
@@ -126,7 +131,11 @@ int socu_refine_solve(const double* L, const double* E, const double* b, double*
                       int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
                       void* workspace, size_t workspace_bytes, double* eta, int32_t* iters, void* stream);
 
-/* Launch object for socu_refine_solve (buffers bound; optional CUDA graph). */
+/* Launch object for socu_refine_solve (buffers bound).  With use_cuda_graph
+ * the refinement rounds are captured in a conditional WHILE graph node that
+ * stops as soon as every instance is done; without it, and in
+ * socu_refine_solve, max_iter rounds are enqueued and finished instances skip
+ * their work. */
 int socu_refine_launch_create(socu_launch_t* out, const double* L, const double* E, const double* b, double* x,
                               const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                               int max_iter, double tol, void* workspace, size_t workspace_bytes, double* eta,

@@ -56,6 +56,7 @@ _SIGNATURES = {
                                   _i64, _i64, _i64, _i64, _int, _vp]),
     "socu_launch_run": (_int, [_vp, _vp]),
     "socu_launch_kernel_count": (_i64, [_vp]),
+    "socu_launch_round_kernel_count": (_i64, [_vp]),
     "socu_launch_destroy": (_int, [_vp]),
     "socu_refine_workspace_bytes": (ctypes.c_size_t, [_i64, _i64, _i64, _i64]),
     "socu_refine_solve": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,

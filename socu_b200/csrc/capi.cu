@@ -288,47 +288,126 @@ RefineArgs refine_args(const double* L, const double* E, const double* b, double
   return a;
 }
 
-// Enqueue (or count) the full mixed solve: init, float factor, max_iter x
-// (float solve, x update, FP64 residual, check).
-int refine_enqueue(const RefineArgs& a, cudaStream_t st, long long* count) {
+// Mixed solve, part 1: state reset, float copies, norms, float factor.
+int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
   const bool run = count == nullptr;
-  long long launches = 0;
   Dims d{a.B, a.N, a.n, a.m, a.S};
-  Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
   Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
-  const int nrc = ceil_div(a.n, kResRows);
-  const size_t sres = smem_residual_elems(a.n) * sizeof(double);
-  const long long nvec = (long long)a.B * a.N * a.n * a.m;
-  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
+    const size_t sres = smem_residual_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
     if (e != cudaSuccess) return cuda_status(e);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
     k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
   }
-  launches += 2;
   long long c = 0;
-  int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c);
+  const int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c);
+  if (count) *count = 2 + c;
+  (void)d;
+  return s;
+}
+
+// Mixed solve, part 2: one refinement round (float solve, x update, FP64
+// residual, convergence test).
+int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
+  const bool run = count == nullptr;
+  Dims d{a.B, a.N, a.n, a.m, a.S};
+  Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
+  const int nrc = ceil_div(a.n, kResRows);
+  const size_t sres = smem_residual_elems(a.n) * sizeof(double);
+  const long long nvec = (long long)a.B * a.N * a.n * a.m;
+  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
+  const int chk_blocks = (a.B + 255) / 256;
+  long long c = 0;
+  const int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c);
   if (s != SOCU_OK) return s;
-  launches += run ? 0 : c;
-  long long cs = 0;
-  if (!run) {
-    s = enqueue<float>(SOCU_OP_SOLVE, pf, nullptr, &cs);
-    if (s != SOCU_OK) return s;
+  if (run) {
+    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+    k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
   }
+  if (count) *count = c + 3;
+  return SOCU_OK;
+}
+
+// Enqueue (or count) the full mixed solve with a fixed max_iter rounds
+// (converged instances skip their work inside each round).
+int refine_enqueue(const RefineArgs& a, cudaStream_t st, long long* count) {
+  const bool run = count == nullptr;
+  long long cp = 0, ci = 0;
+  int s = refine_prologue(a, st, run ? nullptr : &cp);
+  if (s != SOCU_OK) return s;
   for (int it = 0; it < a.max_iter; ++it) {
-    if (run) {
-      s = enqueue<float>(SOCU_OP_SOLVE, pf, st, nullptr);
-      if (s != SOCU_OK) return s;
-      k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
-      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
-      k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
-    }
-    launches += cs + 3;
+    s = refine_iteration(a, st, run ? nullptr : &ci);
+    if (s != SOCU_OK) return s;
+    if (!run) break;
   }
-  if (count) *count = launches;
+  if (count) *count = cp + ci * a.max_iter;
   if (run) return cuda_status(cudaGetLastError());
+  return SOCU_OK;
+}
+
+// Capture the mixed solve into a graph whose refinement rounds sit in a
+// conditional WHILE node: the loop stops as soon as every instance has
+// converged (or hit max_iter), instead of launching max_iter rounds.
+int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
+  cudaStream_t cap = nullptr, body = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking);
+  int st = cuda_status(e);
+  bool capturing = false;
+  if (st == SOCU_OK) {
+    e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    st = cuda_status(e);
+    capturing = st == SOCU_OK;
+  }
+  if (st == SOCU_OK) st = refine_prologue(a, cap, nullptr);
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle hnd = 0;
+  cudaGraphNode_t node = nullptr;
+  cudaGraph_t bodyg = nullptr;
+  if (st == SOCU_OK) {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    e = cudaStreamGetCaptureInfo(cap, &cs, nullptr, &g, &deps, &nd);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = hnd;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &prm);
+    if (e == cudaSuccess) {
+      bodyg = prm.conditional.phGraph_out[0];
+      e = cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies);
+    }
+    st = cuda_status(e);
+  }
+  if (st == SOCU_OK) {
+    e = cudaStreamBeginCaptureToGraph(body, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    st = cuda_status(e);
+    if (st == SOCU_OK) {
+      st = refine_iteration(a, body, nullptr);
+      if (st == SOCU_OK) k_ref_decide<<<1, 1, 0, body>>>(hnd, a.any_active);
+      cudaGraph_t bg = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(body, &bg);
+      if (st == SOCU_OK) st = cuda_status(e2 != cudaSuccess ? e2 : cudaGetLastError());
+    }
+  }
+  cudaGraph_t fin = nullptr;
+  if (capturing) {
+    const cudaError_t e3 = cudaStreamEndCapture(cap, &fin);
+    if (st == SOCU_OK && e3 != cudaSuccess) st = cuda_status(e3);
+  }
+  if (cap) cudaStreamDestroy(cap);
+  if (body) cudaStreamDestroy(body);
+  if (st != SOCU_OK) {
+    if (fin) cudaGraphDestroy(fin);
+    return st;
+  }
+  *out = fin;
   return SOCU_OK;
 }
 }  // namespace
@@ -347,6 +426,7 @@ struct socu_launch_s {
   cudaGraphExec_t exec;
   bool refine = false;
   RefineArgs ra{};
+  long long round_kernels = 0;   // graph WHILE loop: kernels per refinement round
 };
 
 namespace {
@@ -627,6 +707,8 @@ int socu_launch_run(socu_launch_t h, void* stream) {
 
 int64_t socu_launch_kernel_count(socu_launch_t h) { return h ? h->kernels : 0; }
 
+int64_t socu_launch_round_kernel_count(socu_launch_t h) { return h ? h->round_kernels : 0; }
+
 size_t socu_refine_workspace_bytes(int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs) {
   if (batch < 0 || horizon <= 0 || n <= 0 || n_rhs <= 0) return 0;
   return refine_layout(batch, horizon, n, n_rhs).total;
@@ -697,11 +779,21 @@ int socu_refine_launch_create(socu_launch_t* out, const double* L, const double*
   if (batch > 0) refine_enqueue(h->ra, nullptr, &kernels);
   h->kernels = kernels;
   if (use_cuda_graph && batch > 0) {
-    st = capture(h);
+    st = cuda_status(ensure_device(L));
+    if (st == SOCU_OK) st = capture_refine_while(h->ra, &h->graph);
+    if (st == SOCU_OK) st = cuda_status(cudaGraphInstantiate(&h->exec, h->graph, 0));
     if (st != SOCU_OK) {
+      if (h->exec) cudaGraphExecDestroy(h->exec);
+      if (h->graph) cudaGraphDestroy(h->graph);
       delete h;
       return st;
     }
+    // kernels per run: prologue + one round (+ loop control) per round executed
+    long long cp = 0, ci = 0;
+    refine_prologue(h->ra, nullptr, &cp);
+    refine_iteration(h->ra, nullptr, &ci);
+    h->kernels = cp;
+    h->round_kernels = ci + 1;
   }
   (void)stream;
   *out = h;

@@ -255,4 +255,12 @@ __global__ void k_ref_check(RefineArgs a) {
   }
 }
 
+// Loop control for a graph WHILE node: keep iterating while some instance
+// is still active, and clear the flag for the next round.
+__global__ void k_ref_decide(cudaGraphConditionalHandle h, int* any_active) {
+  const int v = *any_active;
+  *any_active = 0;
+  cudaGraphSetConditional(h, v ? 1u : 0u);
+}
+
 }  // namespace socu

@@ -73,6 +73,8 @@ def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_i
     callback.iterations = iters
     callback.workspace_bytes = ws_bytes
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
+    # graph mode: the refinement rounds run in a conditional WHILE node
+    callback.round_kernel_count = int(lib.socu_launch_round_kernel_count(h))
     weakref.finalize(callback, lib.socu_launch_destroy, h)
     return callback
 
