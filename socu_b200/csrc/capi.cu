@@ -118,9 +118,19 @@ Problem<T> make_problem(void* L, void* E, void* x, const uint8_t* mask, const Di
   return p;
 }
 
-// Enqueue (or count, when st == nullptr and count != nullptr) the kernels of one op.
+// Whether a factor may carry its diagonal inverses (k_node<INV>) for
+// matvec-based sweeps: small blocks whose sweeps run resident.
 template <typename T>
-int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count) {
+bool use_inverse(int n, int m) {
+  return n <= 64 && (long long)smem_sweep_res_elems(n, m > 0 ? m : 1) * (long long)sizeof(T) <=
+                        (long long)max_smem_optin();
+}
+
+// Enqueue (or count, when st == nullptr and count != nullptr) the kernels of one op.
+// inv: the factor carries (FACTOR, FACTOR_AND_SOLVE) or has (SOLVE) its
+// diagonal inverses; only for internal factors or within factor_and_solve.
+template <typename T>
+int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, bool inv = false) {
   const std::vector<Level> lv = schedule(p.N);
   const int K = static_cast<int>(lv.size());
   const int n = p.n, nth = threads_for(n);
@@ -131,10 +141,12 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count) 
   const bool res = (long long)smem_sweep_res_elems(n, mm) * (long long)sizeof(T) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, mm) : smem_sweep_elems(n, mm)) * sizeof(T);
   const int nt = ceil_div(n, kTile), nlt = nt * (nt + 1) / 2;
-  auto node_kernel = withY ? k_node<T, true> : k_node<T, false>;
-  auto fwd_kernel = res ? k_fwd<T, true> : k_fwd<T, false>;
+  inv = inv && res && n <= 64;
+  auto node_kernel = withY ? (inv ? k_node<T, true, true> : k_node<T, true, false>)
+                           : (inv ? k_node<T, false, true> : k_node<T, false, false>);
+  auto fwd_kernel = res ? (inv ? k_fwd<T, true, false, true> : k_fwd<T, true>) : k_fwd<T, false>;
   auto pull_kernel = res ? k_fwd<T, true, true> : k_fwd<T, false, true>;
-  auto bwd_kernel = res ? k_bwd<T, true> : k_bwd<T, false>;
+  auto bwd_kernel = res ? (inv ? k_bwd<T, true, true> : k_bwd<T, true>) : k_bwd<T, false>;
   long long launches = 0;
   const bool run = count == nullptr;
 
@@ -226,9 +238,12 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
     const cudaError_t e = ensure_device(L);
     if (e != cudaSuccess) return cuda_status(e);
   }
+  // factor_and_solve keeps the diagonal inverses in the (unspecified) upper
+  // triangles of L and uses them for its own backward sweep
+  const bool inv = op == SOCU_OP_FACTOR_AND_SOLVE;
   if (dtype == SOCU_FLOAT64)
-    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count);
-  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count);
+    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv);
+  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv);
 }
 
 
@@ -302,7 +317,7 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
     k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
   }
   long long c = 0;
-  const int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c);
+  const int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (count) *count = 2 + c;
   (void)d;
   return s;
@@ -320,7 +335,7 @@ int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
   const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
   const int chk_blocks = (a.B + 255) / 256;
   long long c = 0;
-  const int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c);
+  const int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (s != SOCU_OK) return s;
   if (run) {
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
@@ -542,9 +557,11 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   const bool res = (long long)smem_sweep_res_elems(n, a.m) * (long long)sizeof(float) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, a.m) : smem_sweep_elems(n, a.m)) * sizeof(float);
   const size_t sres = smem_residual_elems(n) * sizeof(double);
-  auto fwd = res ? k_fwd<float, true> : k_fwd<float, false>;
-  auto bwd = res ? k_bwd<float, true> : k_bwd<float, false>;
-  cudaError_t e = noalloc_smem(k_node<float, false>, sd);
+  const bool inv = use_inverse<float>(n, a.m);
+  auto node = inv ? k_node<float, false, true> : k_node<float, false, false>;
+  auto fwd = res ? (inv ? k_fwd<float, true, false, true> : k_fwd<float, true>) : k_fwd<float, false>;
+  auto bwd = res ? (inv ? k_bwd<float, true, true> : k_bwd<float, true>) : k_bwd<float, false>;
+  cudaError_t e = noalloc_smem(node, sd);
   if (e == cudaSuccess) e = noalloc_smem(k_update<float>, su);
   if (e == cudaSuccess) e = noalloc_smem(fwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
@@ -560,7 +577,7 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
   k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
   for (int l = 0; l < K; ++l) {
-    k_node<float, false><<<(unsigned)((long long)a.B * lv[l].d), 256, sd, st>>>(pfac, lv[l]);
+    node<<<(unsigned)((long long)a.B * lv[l].d), 256, sd, st>>>(pfac, lv[l]);
     if (l + 1 < K) {
       const long long blocks = (long long)a.B * ((a.N / (2 * lv[l].s)) * nlt + (lv[l].d - 1) * nt * nt);
       if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pfac, lv[l]);

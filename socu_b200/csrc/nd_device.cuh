@@ -278,7 +278,7 @@ __device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restric
 // ---------------------------------------------------------------------------
 // CTA: blocked right-looking Cholesky of the n x n block in A fused with the
 // solve C V = V for nv vectors (columns of V), by 8-column blocks.
-//   1. every thread loads the 8x8 diagonal block into registers and (when
+//   1. every thread loads the diagonal block into registers and (when
 //      FACTOR) factors it redundantly: no communication on the critical chain;
 //   2. one thread per item solves against that block: each row of the panel
 //      below it (A21 <- A21 C11^{-T}) and each vector segment
@@ -286,10 +286,12 @@ __device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restric
 //   3. trailing updates A22 -= P P^T (lower) and V2 -= P V1 with
 //      P = the solved panel (tensor cores for double).
 // FACTOR = false re-runs the solve with an already factored lower(A) = C.
-// On exit lower(A) = C.  Two barriers per 8 columns.
+// On exit lower(A) = C.  Two barriers per block.
 // ---------------------------------------------------------------------------
 template <typename T, bool FACTOR>
 __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
+  // diagonal block width: the whole block lives in every thread's registers
+  // and is factored redundantly by every thread (work grows as BK^3 x threads)
   constexpr int BK = 8;
   for (int K = 0; K < n; K += BK) {
     const int kb = min(BK, n - K);
@@ -343,18 +345,14 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
         if (j < kb) base[j * stride] = x[j];
     }
     __syncthreads();
-    // 3. write the factored diagonal block, then the trailing updates
-    if (FACTOR && threadIdx.x < BK * BK) {
-      const int i = threadIdx.x / BK, j = threadIdx.x % BK;
-      if (i < kb && j <= i) {
-        T v = T(0);
+    // 3. write the factored diagonal block (one thread, static register
+    //    indices), then the trailing updates
+    if (FACTOR && threadIdx.x == 0) {
 #pragma unroll
-        for (int ii = 0; ii < BK; ++ii)
+      for (int i = 0; i < BK; ++i)
 #pragma unroll
-          for (int jj = 0; jj <= ii; ++jj)
-            if (ii == i && jj == j) v = c[ii][jj];
-        A[(K + i) * lda + K + j] = v;
-      }
+        for (int j = 0; j <= i; ++j)
+          if (i < kb) A[(K + i) * lda + K + j] = c[i][j];
     }
     if (R0 < n) {
       const T* P = A + R0 * lda + K;

@@ -36,8 +36,8 @@ __host__ __device__ inline int min_i(int a, int b) { return a < b ? a : b; }
 
 // shared-memory sizes (elements) ------------------------------------------------
 __host__ __device__ inline int gemm_ld(int n, int es) { return es == 8 ? ((n + 15) / 16) * 16 + 4 : n + 1; }
-// vectors solved per pass of k_node: one thread per panel row or vector
-__host__ __device__ inline int node_chunk(int n) { return n <= 64 ? 256 - n : 64; }
+// vectors solved per pass of k_node (items beyond the block size loop)
+__host__ __device__ inline int node_chunk(int n) { return n <= 64 ? 232 : 64; }
 __host__ __device__ inline long long smem_node_elems(int n, int es) {
   return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n), es);
 }
@@ -59,7 +59,10 @@ __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
 //   and, with WITH_Y, the columns of y_i, in passes of node_chunk(n) vectors
 //   (the first pass factors, later passes reuse the factor).
 // ---------------------------------------------------------------------------
-template <typename T, bool WITH_Y>
+// INV: also solve C_i W = I and keep W = C_i^{-1} in the strict upper
+// triangle of L_i (transposed: L_i[c][r] = W[r][c], r > c), for the sweeps
+// that multiply by the inverse (see k_fwd / k_bwd with INV).
+template <typename T, bool WITH_Y, bool INV = false>
 __global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
   constexpr int es = sizeof(T);
   const int b = blockIdx.x / lv.d;
@@ -67,8 +70,8 @@ __global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
   if (!p.active(b)) return;
   const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
   const bool right = i + s < p.N, left = t >= 1;
-  const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0;
-  const int NV = nr + nl + ny;
+  const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0, ni = INV ? n : 0;
+  const int NV = nr + nl + ny + ni;
   const int vc = node_chunk(n), lda = gemm_ld(n, es), ldv = gemm_ld(vc, es);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* A = reinterpret_cast<T*>(smem_raw);
@@ -79,20 +82,32 @@ __global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
   T* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
   T* yi = WITH_Y ? p.Xb(b, i) : nullptr;
 
-  // chunk [v0, v1) of the node's vectors: R rows, then Lf columns, then y columns
+  // chunk [v0, v1) of the node's vectors: R rows, Lf columns, y columns,
+  // then (INV) the columns of the identity
   auto chunk_io = [&](int v0, bool load) {
     const int v1 = min_i(NV, v0 + vc);
     const int rA = v0, rB = min_i(v1, nr);
     const int lS = max(v0, nr), lA = lS - nr, lB = min_i(v1, nr + nl) - nr;
-    const int yS = max(v0, nr + nl), yA = yS - nr - nl, yB = v1 - nr - nl;
+    const int yS = max(v0, nr + nl), yA = yS - nr - nl, yB = min_i(v1, nr + nl + ny) - nr - nl;
+    const int iS = max(v0, nr + nl + ny), iA = iS - nr - nl - ny, iB = v1 - nr - nl - ny;
     if (load) {
       if (rB > rA) async_load_t(V, ldv, R + (long long)rA * n, rB - rA, n, n);
       if (lB > lA) async_load(V + (lS - v0), ldv, Lf + lA, n, lB - lA, n);
       if (yB > yA) async_load(V + (yS - v0), ldv, yi + yA, n, yB - yA, p.m);
+      if (INV && iB > iA)
+        for (int e = threadIdx.x; e < n * (iB - iA); e += blockDim.x) {
+          const int k = e / (iB - iA), j = e - k * (iB - iA);
+          V[k * ldv + (iS - v0) + j] = k == iA + j ? T(1) : T(0);
+        }
     } else {
       if (rB > rA) store_block_t(R + (long long)rA * n, n, V, ldv, rB - rA, n);
       if (lB > lA) store_block(Lf + lA, n, V + (lS - v0), ldv, n, lB - lA);
       if (yB > yA) store_block(yi + yA, p.m, V + (yS - v0), ldv, n, yB - yA);
+      if (INV && iB > iA)   // W[r][c] (r > c) -> L_i[c][r]
+        for (int e = threadIdx.x; e < n * (iB - iA); e += blockDim.x) {
+          const int c = iA + e / n, r = e - (e / n) * n;
+          if (r > c) Li[(long long)c * n + r] = V[r * ldv + (iS - v0) + (c - iA)];
+        }
     }
   };
 
@@ -103,7 +118,8 @@ __global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
   cta_chol_solve<T, true>(A, lda, n, V, ldv, min_i(NV, vc));
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
-    Li[e] = c <= r ? A[r * lda + c] : T(0);
+    if (c <= r) Li[e] = A[r * lda + c];
+    else if (!INV) Li[e] = T(0);
   }
   if (NV > 0) chunk_io(0, false);
   for (int v0 = vc; v0 < NV; v0 += vc) {
@@ -390,8 +406,31 @@ __device__ void res_tri_solve(T* Y, int ldy, int mc, const T* Cs, int ldc, const
 // Every vector has one writer per launch (K launches per forward sweep).
 // RES: factor and coupling blocks resident in shared memory.
 // ---------------------------------------------------------------------------
+// Y_out = W Y (UPPER: W^T Y) with W = C^{-1} kept as in k_node<INV>:
+// W[r][k] = Ls[k][r] (k < r), W[r][r] = dv[r].  Parallel matvec.
+template <typename T, bool UPPER>
+__device__ __forceinline__ void res_inv_apply(T* Yout, const T* Y, int ldy, int mc, const T* Ls, int ldm,
+                                              const T* dv, int n) {
+  for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
+    const int r = o / mc, c = o - r * mc;
+    T s0 = dv[r] * Y[r * ldy + c], s1 = T(0), s2 = T(0), s3 = T(0);
+    const int k0 = UPPER ? r + 1 : 0, k1 = UPPER ? n : r;
+    int k = k0;
+    for (; k + 3 < k1; k += 4) {
+      s0 = fma(UPPER ? Ls[r * ldm + k] : Ls[k * ldm + r], Y[k * ldy + c], s0);
+      s1 = fma(UPPER ? Ls[r * ldm + k + 1] : Ls[(k + 1) * ldm + r], Y[(k + 1) * ldy + c], s1);
+      s2 = fma(UPPER ? Ls[r * ldm + k + 2] : Ls[(k + 2) * ldm + r], Y[(k + 2) * ldy + c], s2);
+      s3 = fma(UPPER ? Ls[r * ldm + k + 3] : Ls[(k + 3) * ldm + r], Y[(k + 3) * ldy + c], s3);
+    }
+    for (; k < k1; ++k) s0 = fma(UPPER ? Ls[r * ldm + k] : Ls[k * ldm + r], Y[k * ldy + c], s0);
+    Yout[r * ldy + c] = (s0 + s1) + (s2 + s3);
+  }
+}
+
 // PULL_ONLY (fused factor_and_solve): apply the updates, never solve.
-template <typename T, bool RES, bool PULL_ONLY = false>
+// INV (resident only): the factor carries its inverse (k_node<INV>), the
+// triangular solve becomes a matvec.
+template <typename T, bool RES, bool PULL_ONLY = false, bool INV = false>
 __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
   const int s = lv.s, N = p.N, n = p.n;
   const int per_b = s == 1 ? lv.d : N / s;
@@ -449,7 +488,15 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
         if (G) res_accumulate<T, true>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G^T y_{j+h}
       }
       __syncthreads();
-      if (solve) res_tri_solve<T, false>(Y, ldy, mc, Cs, ldm, dv, n);
+      if (solve) {
+        if (INV) {
+          res_inv_apply<T, false>(Z2, Y, ldy, mc, Cs, ldm, dv, n);
+          __syncthreads();
+          store_block(yj + c0, p.m, Z2, ldy, n, mc);
+          continue;
+        }
+        res_tri_solve<T, false>(Y, ldy, mc, Cs, ldm, dv, n);
+      }
     } else {
       if (pull) {
         sweep_accumulate<T, false>(Y, Z1, ldy, mc, F, n, Ms);
@@ -464,7 +511,7 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
 // ---------------------------------------------------------------------------
 // k_bwd (level l, descending): x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
 // ---------------------------------------------------------------------------
-template <typename T, bool RES>
+template <typename T, bool RES, bool INV = false>
 __global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
@@ -507,6 +554,12 @@ __global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
       __syncthreads();
       if (left) res_accumulate<T, false>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G x_{i-s}
       __syncthreads();
+      if (INV) {
+        res_inv_apply<T, true>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
+        __syncthreads();
+        store_block(xi + c0, p.m, Z1, ldy, n, mc);
+        continue;
+      }
       res_tri_solve<T, true>(Y, ldy, mc, Cs, ldm, dv, n);
     } else {
       if (right) sweep_accumulate<T, true>(Y, Z1, ldy, mc, F, n, Ms);
