@@ -163,6 +163,17 @@ int socu_refine_solve_noalloc(const double* L, const double* E, const double* b,
                               int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, int max_iter, double tol,
                               double* eta, int32_t* iters, void* stream);
 
+/* Gradient of x = Psi^{-1} b with respect to the blocks of Psi (no counterpart
+ * in the reference, which defines no derivative).  Given x and g = Psi^{-1} gx
+ * (gx = dloss/dx, g obtained with socu_cholesky_solve on the stored factor):
+ *   dD (batch, horizon, n, n): gradient w.r.t. the lower triangle of each D_i
+ *       (the solver reads only lower(D_i)); zeros above the diagonal
+ *   dE (batch, e_blocks, n, n): gradient w.r.t. E_i = Psi_{i+1,i} for
+ *       i < horizon-1, zeros for the remaining storage slots
+ * dloss/db equals g.  One fused kernel. */
+int socu_block_tridiag_grad(socu_dtype dtype, const void* x, const void* g, void* dD, void* dE, int64_t batch,
+                            int64_t horizon, int64_t n, int64_t n_rhs, int64_t e_blocks, void* stream);
+
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */
 int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/socu_b200.h"
+#include "grad.cuh"
 #include "refine.cuh"
 
 namespace socu {
@@ -742,6 +743,35 @@ int socu_refine_solve(const double* L, const double* E, const double* b, double*
   if (e != cudaSuccess) return cuda_status(e);
   const RefineArgs a = refine_args(L, E, b, x, mask, d, max_iter, tol, workspace, eta, iters);
   return refine_enqueue(a, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int socu_block_tridiag_grad(socu_dtype dtype, const void* x, const void* g, void* dD, void* dE, int64_t batch,
+                            int64_t horizon, int64_t n, int64_t n_rhs, int64_t e_blocks, void* stream) {
+  if (dtype != SOCU_FLOAT32 && dtype != SOCU_FLOAT64) return SOCU_ERR_INVALID_ARGUMENT;
+  if (batch < 0 || horizon <= 0 || n <= 0 || n_rhs <= 0 || e_blocks < 0) return SOCU_ERR_INVALID_ARGUMENT;
+  if (e_blocks < horizon - 1) return SOCU_ERR_INVALID_ARGUMENT;
+  if (batch == 0) return SOCU_OK;
+  if (x == nullptr || g == nullptr || dD == nullptr || (e_blocks > 0 && dE == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
+  const size_t es = dtype == SOCU_FLOAT64 ? 8 : 4;
+  const size_t smem = smem_grad_elems((int)n, (int)n_rhs) * es;
+  if ((long long)smem > (long long)max_smem_optin()) return SOCU_ERR_UNSUPPORTED;
+  const long long blocks = batch * (horizon > e_blocks ? horizon : e_blocks);
+  if (!grid_ok(blocks)) return SOCU_ERR_UNSUPPORTED;
+  cudaError_t e = ensure_device(x);
+  if (e != cudaSuccess) return cuda_status(e);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == SOCU_FLOAT64) {
+    GradArgs<double> a{static_cast<const double*>(x), static_cast<const double*>(g), static_cast<double*>(dD),
+                       static_cast<double*>(dE), (int)batch, (int)horizon, (int)n, (int)n_rhs, (int)e_blocks};
+    e = prepare(k_grad<double>, smem);
+    if (e == cudaSuccess) k_grad<double><<<(unsigned)blocks, 256, smem, st>>>(a);
+  } else {
+    GradArgs<float> a{static_cast<const float*>(x), static_cast<const float*>(g), static_cast<float*>(dD),
+                      static_cast<float*>(dE), (int)batch, (int)horizon, (int)n, (int)n_rhs, (int)e_blocks};
+    e = prepare(k_grad<float>, smem);
+    if (e == cudaSuccess) k_grad<float><<<(unsigned)blocks, 256, smem, st>>>(a);
+  }
+  return cuda_status(e != cudaSuccess ? e : cudaGetLastError());
 }
 
 int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,
