@@ -174,6 +174,56 @@ int socu_refine_solve_noalloc(const double* L, const double* E, const double* b,
 int socu_block_tridiag_grad(socu_dtype dtype, const void* x, const void* g, void* dD, void* dE, int64_t batch,
                             int64_t horizon, int64_t n, int64_t n_rhs, int64_t e_blocks, void* stream);
 
+/* ---- ragged batches (no counterpart in the reference, whose launches take
+ * one (N, n, m) shape for the whole batch) ----
+ * `count` independent systems, instance i with horizon[i] blocks of size n[i]
+ * (1..64) and n_rhs[i] right-hand sides, packed back to back: instance i's
+ * L is (horizon[i], n[i], n[i]) at element off_L[i] of one array, its E is
+ * (calculate_off_diag_storage_len(horizon[i]), n[i], n[i]) at off_E[i], its
+ * x/b is (horizon[i], n[i], n_rhs[i]) at off_x[i].  Each instance uses the
+ * layouts and results of socu_cholesky_factor_and_solve.
+ *
+ * socu_ragged_layout: the offsets (arrays of `count`, any may be NULL) and
+ * totals[3] = elements of the packed L, E, x arrays.  Host only. */
+int socu_ragged_layout(const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count,
+                       int64_t* off_L, int64_t* off_E, int64_t* off_x, int64_t* totals);
+
+/* A ragged batch bound to the current device.  All the batch's systems are
+ * solved by one persistent kernel that takes (instance, phase, chunk) tasks
+ * from a device work queue; the queue, the instance descriptors and (refine)
+ * the float workspace are allocated here, once.
+ *   refine = 0: plain factor_and_solve in `dtype`.
+ *   refine = 1: dtype must be SOCU_FLOAT64; float factor + FP64 refinement as
+ *               socu_refine_solve, every instance iterating on its own until
+ *               its eta <= tol or max_iter rounds.
+ * A batch object runs one solve at a time (the queue is shared). */
+typedef struct socu_ragged_s* socu_ragged_t;
+
+int socu_ragged_create(socu_ragged_t* out, socu_dtype dtype, int refine, const int64_t* horizon, const int64_t* n,
+                       const int64_t* n_rhs, int64_t count, int max_iter);
+
+/* Plain path: factor L, E in place and overwrite x (b on input) with the solution. */
+int socu_ragged_factor_and_solve(socu_ragged_t batch, void* L, void* E, void* x, void* stream);
+
+/* Refine path: L, E, b untouched; eta (count,) and iters (count,) as in socu_refine_solve. */
+int socu_ragged_refine_solve(socu_ragged_t batch, const double* L, const double* E, const double* b, double* x,
+                             double tol, double* eta, int32_t* iters, void* stream);
+
+/* Launch object for either path (b, tol, eta, iters only for refine), optionally
+ * captured into a CUDA graph; run and destroy with socu_launch_run /
+ * socu_launch_destroy.  The batch must outlive the launch. */
+int socu_ragged_launch_create(socu_launch_t* out, socu_ragged_t batch, void* L, void* E, const double* b, void* x,
+                              double tol, double* eta, int32_t* iters, int use_cuda_graph, void* stream);
+
+/* Device error word of the last finished solve (synchronises): 0 ok,
+ * 1 a queue wait exceeded its time bound, 2 queue overflow. */
+int socu_ragged_error(socu_ragged_t batch, int* flag);
+
+/* CTAs of the persistent launch (occupancy x SM count). */
+int64_t socu_ragged_grid(socu_ragged_t batch);
+
+int socu_ragged_destroy(socu_ragged_t batch);
+
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */
 int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,

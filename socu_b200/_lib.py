@@ -67,6 +67,15 @@ _SIGNATURES = {
     "socu_block_tridiag_grad": (_int, [_int, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
     "socu_refine_solve_noalloc": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,
                                          _vp, _vp, _vp]),
+    "socu_ragged_layout": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "socu_ragged_create": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _i64, _int]),
+    "socu_ragged_factor_and_solve": (_int, [_vp, _vp, _vp, _vp, _vp]),
+    "socu_ragged_refine_solve": (_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp, _vp]),
+    "socu_ragged_launch_create": (_int, [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp,
+                                         _int, _vp]),
+    "socu_ragged_error": (_int, [_vp, ctypes.POINTER(_int)]),
+    "socu_ragged_grid": (_i64, [_vp]),
+    "socu_ragged_destroy": (_int, [_vp]),
 }
 
 

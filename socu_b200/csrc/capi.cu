@@ -2,6 +2,7 @@
 // and launch objects with optional CUDA-graph capture.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -12,7 +13,7 @@
 
 #include "../../include/socu_b200.h"
 #include "grad.cuh"
-#include "refine.cuh"
+#include "ragged.cuh"
 
 namespace socu {
 namespace {
@@ -431,6 +432,30 @@ int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
 
 using namespace socu;
 
+// A ragged batch: per-instance descriptors, the device work queue and (for
+// the mixed path) the float workspace, all allocated once at creation.
+struct socu_ragged_s {
+  int dtype = SOCU_FLOAT64;
+  bool refine = false;
+  int max_iter = 0;
+  int count = 0;
+  int device = 0;
+  std::vector<RgInst> inst;
+  long long tot[3] = {0, 0, 0};   // elements of the packed L, E, x arrays
+  RgInst* d_inst = nullptr;
+  unsigned long long* d_slot = nullptr;
+  unsigned long long* d_init = nullptr;
+  unsigned int* d_ctr = nullptr;  // head, tail, done
+  int* d_rem = nullptr;
+  int* d_err = nullptr;
+  unsigned int n_init = 0, capacity = 0;
+  float* d_w32 = nullptr;         // refinement: L32 | E32 | R32
+  size_t w_off[3] = {0, 0, 0};
+  RefineState* d_state = nullptr;
+  int vc = 0, grid = 0;
+  size_t smem = 0;
+};
+
 struct socu_launch_s {
   socu_op op;
   socu_dtype dtype;
@@ -443,11 +468,240 @@ struct socu_launch_s {
   bool refine = false;
   RefineArgs ra{};
   long long round_kernels = 0;   // graph WHILE loop: kernels per refinement round
+  socu_ragged_s* rg = nullptr;   // ragged batch (b, tol, eta, iters below for its mixed path)
+  const double* b = nullptr;
+  double tol = 0.0;
+  double* eta = nullptr;
+  int32_t* iters = nullptr;
 };
 
 namespace {
+// ---------------------------------------------------------------------------
+// ragged batches
+// ---------------------------------------------------------------------------
+constexpr int kRgMaxBlock = 64;                 // resident sweeps with diagonal inverses
+constexpr int kRgThreads = 256;
+constexpr long long kRgTimeoutNs = 4000000000LL;   // bound of one queue wait (4 s)
+constexpr size_t kRgNodeSmemBudget = 96 * 1024;
+
+int rg_upc(int n) { return n <= 8 ? 8 : (n <= 16 ? 4 : (n <= 32 ? 2 : 1)); }
+
+// Per-instance descriptors and packed offsets, in instance order.
+int rg_layout(const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count,
+              std::vector<RgInst>* out, long long tot[3]) {
+  if (count < 0) return SOCU_ERR_INVALID_ARGUMENT;
+  if (count >= (1LL << kRgInstBits)) return SOCU_ERR_UNSUPPORTED;
+  if (count > 0 && (horizon == nullptr || n == nullptr || n_rhs == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
+  long long oL = 0, oE = 0, oX = 0;
+  if (out) out->clear();
+  for (int64_t i = 0; i < count; ++i) {
+    if (horizon[i] <= 0 || n[i] <= 0 || n_rhs[i] <= 0) return SOCU_ERR_INVALID_ARGUMENT;
+    if (n[i] > kRgMaxBlock || horizon[i] > (1 << 22) || n_rhs[i] > (1 << 20)) return SOCU_ERR_UNSUPPORTED;
+    RgInst I;
+    I.N = (int)horizon[i];
+    I.n = (int)n[i];
+    I.m = (int)n_rhs[i];
+    I.S = (int)socu_off_diag_storage_len(horizon[i]);
+    I.K = (int)socu_recursive_iterations(horizon[i]);
+    I.upc = rg_upc(I.n);
+    I.oL = oL;
+    I.oE = oE;
+    I.oX = oX;
+    oL += (long long)I.N * I.n * I.n;
+    oE += (long long)I.S * I.n * I.n;
+    oX += (long long)I.N * I.n * I.m;
+    if (out) out->push_back(I);
+  }
+  tot[0] = oL;
+  tot[1] = oE;
+  tot[2] = oX;
+  return SOCU_OK;
+}
+
+void rg_free(socu_ragged_s* r) {
+  cudaFree(r->d_inst);
+  cudaFree(r->d_slot);
+  cudaFree(r->d_init);
+  cudaFree(r->d_ctr);
+  cudaFree(r->d_rem);
+  cudaFree(r->d_err);
+  cudaFree(r->d_w32);
+  cudaFree(r->d_state);
+}
+
+template <typename T, int MODE>
+int rg_prepare_kernel(socu_ragged_s* r) {
+  auto kern = k_ragged<T, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem);
+  int per_sm = 0, sms = 0;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRgThreads, r->smem);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->device);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (per_sm < 1) return SOCU_ERR_UNSUPPORTED;
+  r->grid = per_sm * sms;
+  return SOCU_OK;
+}
+
+int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count) {
+  int st = rg_layout(horizon, n, n_rhs, count, &r->inst, r->tot);
+  if (st != SOCU_OK) return st;
+  r->count = (int)count;
+  if (count == 0) return SOCU_OK;
+  const int mode = r->refine ? kRgRefine : kRgPlain;
+  const int es = r->refine ? 4 : (r->dtype == SOCU_FLOAT64 ? 8 : 4);
+  // queue capacity: every chunk of every phase (max_iter rounds when refining)
+  long long cap = 0;
+  int maxn = 1, maxm = 1, maxnv = 1;
+  for (const RgInst& I : r->inst) {
+    const int phases = r->refine ? rg_refine_phases(I.K, r->max_iter) : rg_plain_phases(I.K);
+    if (phases >= (1 << kRgPhaseBits)) return SOCU_ERR_UNSUPPORTED;
+    for (int ph = 0; ph < phases; ++ph) cap += rg_chunks(rg_phase(I, mode, ph));
+    maxn = std::max(maxn, I.n);
+    maxm = std::max(maxm, I.m);
+    maxnv = std::max(maxnv, 3 * I.n + (r->refine ? 0 : I.m));
+  }
+  // first-phase chunks, largest instances first
+  std::vector<int> order(r->inst.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const RgInst &A = r->inst[a], &B = r->inst[b];
+    return (double)A.N * A.n * A.n * A.n > (double)B.N * B.n * B.n * B.n;
+  });
+  std::vector<unsigned long long> init;
+  for (int i : order) {
+    const int c = rg_chunks(rg_phase(r->inst[i], mode, 0));
+    for (int j = 0; j < c; ++j) init.push_back(rg_encode(i, 0, j));
+  }
+  // shared memory: the largest body at the largest block size
+  const long long lda = gemm_ld(maxn, es);
+  int vc = maxnv;
+  while (vc > 8 && (size_t)((maxn * lda + (long long)maxn * gemm_ld(vc, es)) * es) > kRgNodeSmemBudget) vc -= 8;
+  r->vc = vc;
+  size_t smem = (size_t)(maxn * lda + (long long)maxn * gemm_ld(vc, es)) * es;
+  smem = std::max(smem, (size_t)smem_update_elems(maxn, es) * es);
+  smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
+  if (r->refine) smem = std::max(smem, (size_t)smem_residual_elems(maxn) * sizeof(double));
+  if ((long long)smem > (long long)max_smem_optin()) return SOCU_ERR_UNSUPPORTED;
+  r->smem = smem;
+  cudaError_t e = cudaGetDevice(&r->device);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (r->refine) st = rg_prepare_kernel<float, kRgRefine>(r);
+  else if (r->dtype == SOCU_FLOAT64) st = rg_prepare_kernel<double, kRgPlain>(r);
+  else st = rg_prepare_kernel<float, kRgPlain>(r);
+  if (st != SOCU_OK) return st;
+  cap += r->grid + 64;
+  if (cap >= (1LL << 31)) return SOCU_ERR_UNSUPPORTED;
+  r->capacity = (unsigned)cap;
+  r->n_init = (unsigned)init.size();
+  e = cudaMalloc(&r->d_inst, sizeof(RgInst) * r->inst.size());
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_slot, sizeof(unsigned long long) * r->capacity);
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_init, sizeof(unsigned long long) * init.size());
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_ctr, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_rem, sizeof(int) * r->inst.size());
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_err, sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(r->d_inst, r->inst.data(), sizeof(RgInst) * r->inst.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(r->d_init, init.data(), sizeof(unsigned long long) * init.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(r->d_err, 0, sizeof(int));
+  if (e == cudaSuccess && r->refine) {
+    r->w_off[0] = 0;
+    r->w_off[1] = align256((size_t)r->tot[0] * sizeof(float));
+    r->w_off[2] = r->w_off[1] + align256((size_t)r->tot[1] * sizeof(float));
+    const size_t bytes = r->w_off[2] + align256((size_t)r->tot[2] * sizeof(float));
+    e = cudaMalloc(&r->d_w32, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&r->d_state, sizeof(RefineState) * r->inst.size());
+  }
+  if (e != cudaSuccess) return cuda_status(e);
+  return SOCU_OK;
+}
+
+template <typename T, int MODE>
+int rg_launch(socu_ragged_s* r, RgArgs<T> a, cudaStream_t st) {
+  a.inst = r->d_inst;
+  a.count = r->count;
+  a.q.slot = r->d_slot;
+  a.q.head = r->d_ctr;
+  a.q.tail = r->d_ctr + 1;
+  a.q.done = r->d_ctr + 2;
+  a.q.rem = r->d_rem;
+  a.q.error = r->d_err;
+  a.q.init = r->d_init;
+  a.q.n_init = r->n_init;
+  a.q.capacity = r->capacity;
+  a.vc = r->vc;
+  a.timeout_ns = kRgTimeoutNs;
+  cudaError_t e = cudaMemsetAsync(r->d_slot + r->n_init, 0,
+                                  sizeof(unsigned long long) * (r->capacity - r->n_init), st);
+  if (e != cudaSuccess) return cuda_status(e);
+  const long long work = std::max<long long>(r->n_init, r->count);
+  const int sb = (int)std::min<long long>((work + 255) / 256, 1024);
+  k_rg_start<T, MODE><<<sb, 256, 0, st>>>(a);
+  k_ragged<T, MODE><<<r->grid, kRgThreads, r->smem, st>>>(a);
+  return cuda_status(cudaGetLastError());
+}
+
+int rg_device(const socu_ragged_s* r) {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != r->device) return cuda_status(cudaSetDevice(r->device));
+  return SOCU_OK;
+}
+
+int rg_factor_and_solve(socu_ragged_s* r, void* L, void* E, void* x, cudaStream_t st) {
+  if (r->refine) return SOCU_ERR_INVALID_ARGUMENT;
+  if (r->count == 0) return SOCU_OK;
+  if (L == nullptr || x == nullptr || (r->tot[1] > 0 && E == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
+  int s = rg_device(r);
+  if (s != SOCU_OK) return s;
+  if (r->dtype == SOCU_FLOAT64) {
+    RgArgs<double> a{};
+    a.L = static_cast<double*>(L);
+    a.E = static_cast<double*>(E);
+    a.X = static_cast<double*>(x);
+    return rg_launch<double, kRgPlain>(r, a, st);
+  }
+  RgArgs<float> a{};
+  a.L = static_cast<float*>(L);
+  a.E = static_cast<float*>(E);
+  a.X = static_cast<float*>(x);
+  return rg_launch<float, kRgPlain>(r, a, st);
+}
+
+int rg_refine_solve(socu_ragged_s* r, const double* L, const double* E, const double* b, double* x, double tol,
+                    double* eta, int32_t* iters, cudaStream_t st) {
+  if (!r->refine || !(tol >= 0.0)) return SOCU_ERR_INVALID_ARGUMENT;
+  if (r->count == 0) return SOCU_OK;
+  if (L == nullptr || b == nullptr || x == nullptr || eta == nullptr || iters == nullptr ||
+      (r->tot[1] > 0 && E == nullptr))
+    return SOCU_ERR_INVALID_ARGUMENT;
+  int s = rg_device(r);
+  if (s != SOCU_OK) return s;
+  char* w = reinterpret_cast<char*>(r->d_w32);
+  RgArgs<float> a{};
+  a.L = reinterpret_cast<float*>(w + r->w_off[0]);
+  a.E = reinterpret_cast<float*>(w + r->w_off[1]);
+  a.X = reinterpret_cast<float*>(w + r->w_off[2]);
+  a.L64 = L;
+  a.E64 = E;
+  a.b64 = b;
+  a.x64 = x;
+  a.st = r->d_state;
+  a.eta = eta;
+  a.iters = iters;
+  a.tol = tol;
+  a.max_iter = r->max_iter;
+  return rg_launch<float, kRgRefine>(r, a, st);
+}
+
 // enqueue one run of a launch object on `st`
 int launch_enqueue(socu_launch_s* h, cudaStream_t st) {
+  if (h->rg) {
+    if (h->rg->refine)
+      return rg_refine_solve(h->rg, static_cast<const double*>(h->L), static_cast<const double*>(h->E), h->b,
+                             static_cast<double*>(h->x), h->tol, h->eta, h->iters, st);
+    return rg_factor_and_solve(h->rg, h->L, h->E, h->x, st);
+  }
   if (h->refine) {
     if (h->batch == 0) return SOCU_OK;
     const cudaError_t e = ensure_device(h->L);
@@ -460,8 +714,13 @@ int launch_enqueue(socu_launch_s* h, cudaStream_t st) {
 // Capture one run into a CUDA graph on a private stream (the legacy default
 // stream cannot capture) and instantiate it eagerly.
 int capture(socu_launch_s* h) {
-  const cudaError_t ed = ensure_device(h->L);
-  if (ed != cudaSuccess) return cuda_status(ed);
+  if (h->rg) {
+    const int sd = rg_device(h->rg);
+    if (sd != SOCU_OK) return sd;
+  } else {
+    const cudaError_t ed = ensure_device(h->L);
+    if (ed != cudaSuccess) return cuda_status(ed);
+  }
   cudaStream_t cap = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
   int st = SOCU_OK;
@@ -876,6 +1135,117 @@ int socu_refine_solve_noalloc(const double* L, const double* E, const double* b,
   if (st != SOCU_OK) return st;
   const RefineArgs a = refine_args(L, E, b, x, mask, d, max_iter, tol, scratch, eta, iters);
   return refine_enqueue_noalloc(a, static_cast<cudaStream_t>(stream));
+}
+
+// ---------------------------------------------------------------------------
+// ragged batches
+// ---------------------------------------------------------------------------
+int socu_ragged_layout(const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count,
+                       int64_t* off_L, int64_t* off_E, int64_t* off_x, int64_t* totals) {
+  std::vector<RgInst> inst;
+  long long tot[3];
+  const int st = rg_layout(horizon, n, n_rhs, count, &inst, tot);
+  if (st != SOCU_OK) return st;
+  for (int64_t i = 0; i < count; ++i) {
+    if (off_L) off_L[i] = inst[i].oL;
+    if (off_E) off_E[i] = inst[i].oE;
+    if (off_x) off_x[i] = inst[i].oX;
+  }
+  if (totals) {
+    totals[0] = tot[0];
+    totals[1] = tot[1];
+    totals[2] = tot[2];
+  }
+  return SOCU_OK;
+}
+
+int socu_ragged_create(socu_ragged_t* out, socu_dtype dtype, int refine, const int64_t* horizon, const int64_t* n,
+                       const int64_t* n_rhs, int64_t count, int max_iter) {
+  if (out == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (dtype != SOCU_FLOAT32 && dtype != SOCU_FLOAT64) return SOCU_ERR_INVALID_ARGUMENT;
+  if (refine && (dtype != SOCU_FLOAT64 || max_iter < 1 || max_iter > 1000)) return SOCU_ERR_INVALID_ARGUMENT;
+  socu_ragged_s* r = new (std::nothrow) socu_ragged_s();
+  if (!r) return SOCU_ERR_UNSUPPORTED;
+  r->dtype = dtype;
+  r->refine = refine != 0;
+  r->max_iter = refine ? max_iter : 0;
+  const int st = rg_create(r, horizon, n, n_rhs, count);
+  if (st != SOCU_OK) {
+    rg_free(r);
+    delete r;
+    return st;
+  }
+  *out = r;
+  return SOCU_OK;
+}
+
+int socu_ragged_factor_and_solve(socu_ragged_t r, void* L, void* E, void* x, void* stream) {
+  if (r == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  return rg_factor_and_solve(r, L, E, x, static_cast<cudaStream_t>(stream));
+}
+
+int socu_ragged_refine_solve(socu_ragged_t r, const double* L, const double* E, const double* b, double* x,
+                             double tol, double* eta, int32_t* iters, void* stream) {
+  if (r == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  return rg_refine_solve(r, L, E, b, x, tol, eta, iters, static_cast<cudaStream_t>(stream));
+}
+
+int socu_ragged_launch_create(socu_launch_t* out, socu_ragged_t r, void* L, void* E, const double* b, void* x,
+                              double tol, double* eta, int32_t* iters, int use_cuda_graph, void* stream) {
+  if (out == nullptr || r == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (r->count > 0) {
+    if (L == nullptr || x == nullptr || (r->tot[1] > 0 && E == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
+    if (r->refine && (b == nullptr || eta == nullptr || iters == nullptr || !(tol >= 0.0)))
+      return SOCU_ERR_INVALID_ARGUMENT;
+  }
+  socu_launch_s* h = new (std::nothrow) socu_launch_s();
+  if (!h) return SOCU_ERR_UNSUPPORTED;
+  h->op = SOCU_OP_FACTOR_AND_SOLVE;
+  h->dtype = r->refine ? SOCU_FLOAT64 : (socu_dtype)r->dtype;
+  h->L = L;
+  h->E = E;
+  h->x = x;
+  h->mask = nullptr;
+  h->batch = r->count;
+  h->graph = nullptr;
+  h->exec = nullptr;
+  h->rg = r;
+  h->b = b;
+  h->tol = tol;
+  h->eta = eta;
+  h->iters = iters;
+  h->kernels = r->count > 0 ? 2 : 0;
+  if (use_cuda_graph && r->count > 0) {
+    const int st = capture(h);
+    if (st != SOCU_OK) {
+      delete h;
+      return st;
+    }
+  }
+  (void)stream;
+  *out = h;
+  return SOCU_OK;
+}
+
+int socu_ragged_error(socu_ragged_t r, int* flag) {
+  if (r == nullptr || flag == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *flag = 0;
+  if (r->count == 0) return SOCU_OK;
+  int s = rg_device(r);
+  if (s != SOCU_OK) return s;
+  return cuda_status(cudaMemcpy(flag, r->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+}
+
+int64_t socu_ragged_grid(socu_ragged_t r) { return r ? r->grid : 0; }
+
+int socu_ragged_destroy(socu_ragged_t r) {
+  if (r == nullptr) return SOCU_OK;
+  if (r->count > 0) rg_device(r);
+  rg_free(r);
+  delete r;
+  return SOCU_OK;
 }
 
 }  // extern "C"

@@ -62,18 +62,17 @@ __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
 // INV: also solve C_i W = I and keep W = C_i^{-1} in the strict upper
 // triangle of L_i (transposed: L_i[c][r] = W[r][c], r > c), for the sweeps
 // that multiply by the inverse (see k_fwd / k_bwd with INV).
-template <typename T, bool WITH_Y, bool INV = false>
-__global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
+// Body of one node (instance b, level node t) with vc vectors per pass; the
+// shared buffer holds n*gemm_ld(n) + n*gemm_ld(vc) elements.
+template <typename T, bool WITH_Y, bool INV>
+__device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, int b, int t,
+                                          unsigned char* smem_raw, int vc) {
   constexpr int es = sizeof(T);
-  const int b = blockIdx.x / lv.d;
-  const int t = blockIdx.x - b * lv.d;
-  if (!p.active(b)) return;
   const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
   const bool right = i + s < p.N, left = t >= 1;
   const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0, ni = INV ? n : 0;
   const int NV = nr + nl + ny + ni;
-  const int vc = node_chunk(n), lda = gemm_ld(n, es), ldv = gemm_ld(vc, es);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lda = gemm_ld(n, es), ldv = gemm_ld(vc, es);
   T* A = reinterpret_cast<T*>(smem_raw);
   T* V = A + n * lda;
 
@@ -132,6 +131,15 @@ __global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
   }
 }
 
+template <typename T, bool WITH_Y, bool INV = false>
+__global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
+  const int b = blockIdx.x / lv.d;
+  const int t = blockIdx.x - b * lv.d;
+  if (!p.active(b)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n));
+}
+
 // ---------------------------------------------------------------------------
 // k_update
 // ---------------------------------------------------------------------------
@@ -142,20 +150,22 @@ __device__ __forceinline__ void lower_tile_index(int lt, int& ta, int& tc) {
   tc = lt - a * (a + 1) / 2;
 }
 
+// Number of output tiles of one update level per instance: U targets with
+// nlt lower tiles each, then d-1 fill-in blocks with nt*nt tiles each.
+__host__ __device__ inline int update_tiles(int n, int N, const Level& lv) {
+  const int nt = ceil_div(n, kTile);
+  return (N / (2 * lv.s)) * (nt * (nt + 1) / 2) + (lv.d - 1) * nt * nt;
+}
+
+// Body of one output tile `task` in [0, update_tiles) of instance b.
 template <typename T>
-__global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
+__device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv, int b, int task,
+                                            unsigned char* smem_raw) {
   constexpr int es = sizeof(T);
   const int n = p.n, N = p.N, s = lv.s;
   const int nt = ceil_div(n, kTile);
   const int nlt = nt * (nt + 1) / 2;
   const int U = N / (2 * s);
-  const int nfill = lv.d - 1;
-  const int per_b = U * nlt + nfill * nt * nt;
-  const int b = blockIdx.x / per_b;
-  const int task = blockIdx.x - b * per_b;
-  if (!p.active(b)) return;
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Ab = reinterpret_cast<T*>(smem_raw);
 
   if (task < U * nlt) {
@@ -209,6 +219,16 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
     cta_gemm<T, false, false>(wa, wc, n, Ab, lda, Bb, ldg,
                               [&](int r, int c, T v) { X[(long long)(r0 + r) * n + c0 + c] -= v; });
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
+  const int per_b = update_tiles(p.n, p.N, lv);
+  const int b = blockIdx.x / per_b;
+  const int task = blockIdx.x - b * per_b;
+  if (!p.active(b)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  update_body<T>(p, lv, b, task, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -430,13 +450,13 @@ __device__ __forceinline__ void res_inv_apply(T* Yout, const T* Y, int ldy, int 
 // PULL_ONLY (fused factor_and_solve): apply the updates, never solve.
 // INV (resident only): the factor carries its inverse (k_node<INV>), the
 // triangular solve becomes a matvec.
-template <typename T, bool RES, bool PULL_ONLY = false, bool INV = false>
-__global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
+// Tasks of one forward level per instance.
+__host__ __device__ inline int fwd_tasks(int N, const Level& lv) { return lv.s == 1 ? lv.d : N / lv.s; }
+
+template <typename T, bool RES, bool PULL_ONLY, bool INV>
+__device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, int b, int task,
+                                         unsigned char* smem_raw) {
   const int s = lv.s, N = p.N, n = p.n;
-  const int per_b = s == 1 ? lv.d : N / s;
-  const int b = blockIdx.x / per_b;
-  const int task = blockIdx.x - b * per_b;
-  if (!p.active(b)) return;
   const int h = s / 2;
   int j;
   bool pull, solve;
@@ -453,7 +473,6 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
     F = p.Eb(b, lv.op + 2 * u - 2);
     if (j + h < N) G = p.Eb(b, lv.op + 2 * u - 1);
   }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
@@ -508,17 +527,24 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
   }
 }
 
+template <typename T, bool RES, bool PULL_ONLY = false, bool INV = false>
+__global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
+  const int per_b = fwd_tasks(p.N, lv);
+  const int b = blockIdx.x / per_b;
+  const int task = blockIdx.x - b * per_b;
+  if (!p.active(b)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fwd_body<T, RES, PULL_ONLY, INV>(p, lv, b, task, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // k_bwd (level l, descending): x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
 // ---------------------------------------------------------------------------
-template <typename T, bool RES, bool INV = false>
-__global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
-  const int b = blockIdx.x / lv.d;
-  const int t = blockIdx.x - b * lv.d;
-  if (!p.active(b)) return;
+template <typename T, bool RES, bool INV>
+__device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, int b, int t,
+                                         unsigned char* smem_raw) {
   const int n = p.n, s = lv.s, N = p.N;
   const int i = s - 1 + 2 * s * t;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
@@ -568,6 +594,15 @@ __global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
     }
     store_block(xi + c0, p.m, Y, ldy, n, mc);
   }
+}
+
+template <typename T, bool RES, bool INV = false>
+__global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
+  const int b = blockIdx.x / lv.d;
+  const int t = blockIdx.x - b * lv.d;
+  if (!p.active(b)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  bwd_body<T, RES, INV>(p, lv, b, t, smem_raw);
 }
 
 }  // namespace socu

@@ -76,15 +76,10 @@ __global__ void k_ref_reset(RefineArgs a) {
 
 // One CTA per (instance, block index i < max(N, S)): float copies of L_i and
 // slot i, R32 = b, x = 0, ||Psi||_inf and ||b||_inf contributions of block row i.
-__global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
-  const int per = a.N > a.S ? a.N : a.S;
-  const int bi = blockIdx.x / per;
-  const int i = blockIdx.x - bi * per;
+__device__ __forceinline__ void ref_init_body(const RefineArgs& a, int bi, int i) {
   __shared__ double red[32];
-  const bool on = a.mask == nullptr || a.mask[bi] != 0;
   const int n = a.n, m = a.m;
   const long long nn = (long long)n * n;
-  if (!on) return;
   if (i < a.N) {
     const double* Li = a.L + ((long long)bi * a.N + i) * nn;
     float* L32 = a.L32 + ((long long)bi * a.N + i) * nn;
@@ -130,6 +125,14 @@ __global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
+  const int per = a.N > a.S ? a.N : a.S;
+  const int bi = blockIdx.x / per;
+  const int i = blockIdx.x - bi * per;
+  if (a.mask != nullptr && a.mask[bi] == 0) return;
+  ref_init_body(a, bi, i);
+}
+
 // x += delta (R32) for active instances; grid-stride over the whole batch.
 __global__ void __launch_bounds__(256) k_ref_update(RefineArgs a) {
   const long long per = (long long)a.N * a.n * a.m;
@@ -154,17 +157,9 @@ __host__ __device__ inline long long smem_residual_elems(int n) {
 // REFINE: write R32 = float(r), accumulate norms, skip inactive instances.
 // Otherwise write r (double) to a.rout for every instance.
 template <bool REFINE>
-__global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
+__device__ __forceinline__ void residual_body(const RefineArgs& a, int bi, int i, int r0, unsigned char* smem_raw) {
   const int n = a.n, m = a.m, N = a.N;
-  const int nrc = (n + kResRows - 1) / kResRows;
-  const int per = N * nrc;
-  const int bi = blockIdx.x / per;
-  const int rem = blockIdx.x - bi * per;
-  const int i = rem / nrc;
-  const int r0 = (rem - i * nrc) * kResRows;
   const int rw = min(kResRows, n - r0);
-  if (REFINE && !a.active[bi]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ldn = n + 1, ldc = kResRows + 1, ldx = kResCols + 1;
   double* Lr = reinterpret_cast<double*>(smem_raw);
   double* Er = Lr + kResRows * ldn;
@@ -224,6 +219,18 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
       atomic_max_pos(&a.st[bi].xnorm, xm);
     }
   }
+}
+
+template <bool REFINE>
+__global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
+  const int nrc = (a.n + kResRows - 1) / kResRows;
+  const int per = a.N * nrc;
+  const int bi = blockIdx.x / per;
+  const int rem = blockIdx.x - bi * per;
+  const int i = rem / nrc;
+  if (REFINE && !a.active[bi]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  residual_body<REFINE>(a, bi, i, (rem - i * nrc) * kResRows, smem_raw);
 }
 
 // Convergence test per instance; clears the accumulators for the next round.
