@@ -38,7 +38,19 @@ def storage_len(N):
     return sum(N // (2 ** l) - 1 for l in range(N.bit_length()))
 
 
-def make_problem():
+RAGGED_COUNT, RAGGED_SEED = 4096, 0
+RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
+                   "instance i seeded with 0 + i, one persistent launch per solve")
+
+
+def make_problem_gpu(dev):
+    """The workload system on the device (README construction, torch generator)."""
+    from socu_b200.problems import readme_blocks
+    return readme_blocks(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED, batch=1, device=dev)
+
+
+def make_problem_host():
+    """The workload system on the host for the reference arm (NumPy generator, same construction)."""
     from oracle.generators import readme_problem
     return readme_problem(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED)
 
@@ -128,7 +140,7 @@ def cpu_oracle_solves_per_s(L, E, b, reps):
 def run_reference(args, rank):
     if rank != 0:
         return
-    L, E, b = make_problem()
+    L, E, b = make_problem_host()
     cores = len(os.sched_getaffinity(0))
     from oracle import nd_cholesky as nd
     for _ in range(args.warmup):
@@ -168,10 +180,7 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    L_np, E_np, b_np = make_problem()
-    L0 = torch.tensor(L_np, device=dev)
-    E0 = torch.tensor(E_np, device=dev)
-    b0 = torch.tensor(b_np, device=dev)
+    L0, E0, b0 = make_problem_gpu(dev)
     x = torch.zeros_like(b0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 
@@ -208,15 +217,16 @@ def run_ours(args, rank, world, local_rank):
         L32w.copy_(L32); E32w.copy_(E32)
 
     nothing = lambda: None
+    # clocks are sampled over the whole measurement window (every timed region
+    # below); nvidia-smi needs about a second before its first sample
+    sampler = ClockSampler(local_rank)
+    sampler.__enter__()
+    time.sleep(1.5)
     for _ in range(args.warmup):
         mixed(); reset_plain(); plain(); reset_fac(); fac32()
     barrier()
-
-    sampler = ClockSampler(local_rank)
-    with sampler:
-        barrier()
-        t_mixed = time_steps(mixed, nothing, args.steps)
-        barrier()
+    t_mixed = time_steps(mixed, nothing, args.steps)
+    barrier()
     t_plain = time_steps(plain, reset_plain, args.steps)
     t_fac = time_steps(fac32, reset_fac, args.steps)
     barrier()
@@ -251,6 +261,11 @@ def run_ours(args, rank, world, local_rank):
         return float(v)
 
     sec_mixed, sec_plain, sec_fac, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_fac), agg(t_e2e)
+    del e2e_run, Ld, Ed, bd, xd, Lw, Ew, xw, L32, E32, L32w, E32w
+    torch.cuda.empty_cache()
+    rg = bench_ragged(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
+    barrier()
+    sampler.__exit__(None, None, None)
     if rank != 0:
         return
     n, N, m = BLOCK, N_BLOCKS, NRHS
@@ -262,7 +277,7 @@ def run_ours(args, rank, world, local_rank):
         hbm_peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     achieved = fac_bytes / sec_fac / 1e9
     cores = len(os.sched_getaffinity(0))
-    cpu_v, cpu_ts = cpu_oracle_solves_per_s(L_np, E_np, b_np, reps=2)
+    cpu_v, cpu_ts = cpu_oracle_solves_per_s(L0[0].cpu().numpy(), E0[0].cpu().numpy(), b0[0].cpu().numpy(), reps=2)
     value = world / sec_mixed
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -286,9 +301,60 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": world / sec_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": sec_e2e * 1e3},
         "gpu_launches": (mixed.kernel_count + abs(iters) * mixed.round_kernel_count) * args.steps,
-        "clocks": sampler.summary(),
+        "clocks": dict(sampler.summary(), window="100 ms samples over all timed regions of this run "
+                                                  "(workload, e2e, ragged) and their warm-ups"),
     }
+    if rg is not None:
+        line["ragged"] = rg
     print(json.dumps(line), flush=True)
+
+
+def bench_ragged(dev, steps, time_steps, agg):
+    """Uneven MPC-style batch in one persistent launch: FP64 plain and float
+    factor + FP64 refinement.  The packed inputs (several GB) exceed L2."""
+    import torch
+
+    from socu_b200.problems import fill_ragged, ragged_shapes
+    from socu_b200.ragged import (RaggedBatch, create_ragged_factor_and_solve_launch,
+                                  create_ragged_refined_solve_launch)
+
+    Ns, ns, ms = ragged_shapes(RAGGED_SEED, RAGGED_COUNT)
+    plain_b = RaggedBatch(Ns, ns, ms, dtype=torch.float64, device=dev)
+    L, E, b = plain_b.empty()
+    fill_ragged(plain_b, L, E, b, seed=RAGGED_SEED)
+    mixed_b = RaggedBatch(Ns, ns, ms, dtype=torch.float64, device=dev, refine=True, max_iter=MAX_ITER)
+    x = torch.zeros_like(b)
+    run_m = create_ragged_refined_solve_launch(mixed_b, L, E, b, x, tol=TOL)
+    Lw, Ew, xw = L.clone(), E.clone(), b.clone()
+    run_p = create_ragged_factor_and_solve_launch(plain_b, Lw, Ew, xw)
+
+    def reset():
+        Lw.copy_(L); Ew.copy_(E); xw.copy_(b)
+
+    for _ in range(2):
+        run_m(); reset(); run_p()
+    torch.cuda.synchronize(dev)
+    k = max(3, steps // 2)
+    t_m = time_steps(run_m, lambda: None, k)
+    t_p = time_steps(run_p, reset, k)
+    errs = (mixed_b.error_flag(), plain_b.error_flag())
+    sec_m, sec_p = agg(t_m), agg(t_p)
+    flops = sum(algorithmic_factor_flops(int(N), int(n)) for N, n in zip(Ns, ns))
+    out = {
+        "workload": RAGGED_WORKLOAD,
+        "mixed_refine": {"value": RAGGED_COUNT / sec_m, "unit": "solves/s", "ms_per_step": sec_m * 1e3,
+                         "eta_max": float(run_m.eta.max()), "iterations_max": int(run_m.iterations.max()),
+                         "iterations_mean": float(run_m.iterations.double().mean())},
+        "fp64_plain": {"value": RAGGED_COUNT / sec_p, "unit": "solves/s", "ms_per_step": sec_p * 1e3,
+                       "factor_gflops": flops / sec_p / 1e9},
+        "mixed_over_fp64": sec_p / sec_m,
+        "persistent_ctas": plain_b.grid,
+        "queue_errors": list(errs),
+        "packed_bytes_fp64": (L.numel() + E.numel() + 2 * b.numel()) * 8,
+        "gpu_launches_per_solve": 2,
+    }
+    del run_m, run_p, L, E, b, x, Lw, Ew, xw
+    return out
 
 
 def main():
@@ -297,6 +363,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
