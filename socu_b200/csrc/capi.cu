@@ -137,12 +137,12 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   const int K = static_cast<int>(lv.size());
   const int n = p.n, nth = threads_for(n);
   const bool withY = op == SOCU_OP_FACTOR_AND_SOLVE;
-  const size_t sd = smem_node_elems(n, sizeof(T)) * sizeof(T);
-  const size_t su = smem_update_elems(n, sizeof(T)) * sizeof(T);
+  const size_t sd = smem_node_launch_elems(n, withY ? p.m : 0, sizeof(T)) * sizeof(T);
+  const size_t su = smem_update_launch_elems(n, sizeof(T)) * sizeof(T);
   const int mm = p.m > 0 ? p.m : 1;
   const bool res = (long long)smem_sweep_res_elems(n, mm) * (long long)sizeof(T) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, mm) : smem_sweep_elems(n, mm)) * sizeof(T);
-  const int nt = ceil_div(n, kTile), nlt = nt * (nt + 1) / 2;
+  (void)0;
   inv = inv && res && n <= 64;
   auto node_kernel = withY ? (inv ? k_node<T, true, true> : k_node<T, true, false>)
                            : (inv ? k_node<T, false, true> : k_node<T, false, false>);
@@ -174,10 +174,10 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   if (factor) {
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
-      go(node_kernel, (long long)p.B * L.d, sd, L, 256);
+      go(node_kernel, (long long)p.B * L.d, sd, L, nth);
       if (l + 1 < K) {
         const int U = p.N / (2 * L.s);
-        go(k_update<T>, (long long)p.B * (U * nlt + (L.d - 1) * nt * nt), su, L);
+        go(k_update<T>, (long long)p.B * update_launch_tasks(n, p.N, L), su, L);
         // fused forward: apply this level's updates to every target vector
         if (withY) go(pull_kernel, (long long)p.B * (p.N / lv[l + 1].s), ss, lv[l + 1]);
       }
@@ -482,7 +482,6 @@ namespace {
 constexpr int kRgMaxBlock = 64;                 // resident sweeps with diagonal inverses
 constexpr int kRgThreads = 256;
 constexpr long long kRgTimeoutNs = 4000000000LL;   // bound of one queue wait (4 s)
-constexpr size_t kRgNodeSmemBudget = 96 * 1024;
 
 int rg_upc(int n) { return n <= 8 ? 8 : (n <= 16 ? 4 : (n <= 32 ? 2 : 1)); }
 
@@ -572,13 +571,11 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
     const int c = rg_chunks(rg_phase(r->inst[i], mode, 0));
     for (int j = 0; j < c; ++j) init.push_back(rg_encode(i, 0, j));
   }
-  // shared memory: the largest body at the largest block size
-  const long long lda = gemm_ld(maxn, es);
-  int vc = maxnv;
-  while (vc > 8 && (size_t)((maxn * lda + (long long)maxn * gemm_ld(vc, es)) * es) > kRgNodeSmemBudget) vc -= 8;
-  r->vc = vc;
-  size_t smem = (size_t)(maxn * lda + (long long)maxn * gemm_ld(vc, es)) * es;
-  smem = std::max(smem, (size_t)smem_update_elems(maxn, es) * es);
+  // shared memory: the largest body at the largest block size (n <= 64: the
+  // inverse-first node body)
+  r->vc = maxnv;
+  size_t smem = (size_t)smem_node_gemm_elems(maxn, r->refine ? 0 : maxm, es) * es;
+  smem = std::max(smem, (size_t)smem_update_full_elems(maxn, es) * es);
   smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
   if (r->refine) smem = std::max(smem, (size_t)smem_residual_elems(maxn) * sizeof(double));
   if ((long long)smem > (long long)max_smem_optin()) return SOCU_ERR_UNSUPPORTED;
@@ -812,8 +809,8 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   const Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
   const Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
   const int n = a.n, nth = threads_for(n);
-  const size_t sd = smem_node_elems(n, sizeof(float)) * sizeof(float);
-  const size_t su = smem_update_elems(n, sizeof(float)) * sizeof(float);
+  const size_t sd = smem_node_launch_elems(n, 0, sizeof(float)) * sizeof(float);
+  const size_t su = smem_update_launch_elems(n, sizeof(float)) * sizeof(float);
   const bool res = (long long)smem_sweep_res_elems(n, a.m) * (long long)sizeof(float) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, a.m) : smem_sweep_elems(n, a.m)) * sizeof(float);
   const size_t sres = smem_residual_elems(n) * sizeof(double);
@@ -827,7 +824,7 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
   if (e != cudaSuccess) return cuda_status(e);
-  const int nt = ceil_div(n, kTile), nlt = nt * (nt + 1) / 2;
+  (void)0;
   const int nrc = ceil_div(n, kResRows);
   const long long nvec = (long long)a.B * a.N * a.n * a.m;
   const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
@@ -837,9 +834,9 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
   k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
   for (int l = 0; l < K; ++l) {
-    node<<<(unsigned)((long long)a.B * lv[l].d), 256, sd, st>>>(pfac, lv[l]);
+    node<<<(unsigned)((long long)a.B * lv[l].d), nth, sd, st>>>(pfac, lv[l]);
     if (l + 1 < K) {
-      const long long blocks = (long long)a.B * ((a.N / (2 * lv[l].s)) * nlt + (lv[l].d - 1) * nt * nt);
+      const long long blocks = (long long)a.B * update_launch_tasks(n, a.N, lv[l]);
       if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pfac, lv[l]);
     }
   }

@@ -9,9 +9,12 @@
 // (socu/block_tridiag_solver.py:174).  Slot E[o_l + k] couples node
 // p = (k+1)s-1 (columns) with q = p+s (rows).
 //
-// Factor output: lower(L_i) = C_i (lower Cholesky factor), upper(L_i) = 0.
-// The reference leaves the upper triangle unspecified; every kernel here reads
-// only lower(L_i), so factors are interchangeable with socu's.
+// Factor output: lower(L_i) = C_i (lower Cholesky factor).  The strict upper
+// triangle is 0, or holds W_i^T with W_i = C_i^{-1} where a path keeps the
+// diagonal inverses (factor_and_solve, the internal float factor of the mixed
+// solve).  The reference leaves the upper triangle unspecified and every
+// kernel here that is given a factor from outside reads only lower(L_i), so
+// factors are interchangeable with socu's.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -296,8 +299,11 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
   for (int K = 0; K < n; K += BK) {
     const int kb = min(BK, n - K);
     const int R0 = K + kb, rows = FACTOR ? n - R0 : 0;
-    // 1. diagonal block in registers (identity-padded past kb)
+    // 1. diagonal block in registers (identity-padded past kb), only in the
+    //    threads that own an item (thread 0 always: it writes the block back)
     T c[BK][BK], rsv[BK];
+    const bool act = threadIdx.x < max(rows + nv, 1);
+    if (act) {
 #pragma unroll
     for (int i = 0; i < BK; ++i)
 #pragma unroll
@@ -343,6 +349,7 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
 #pragma unroll
       for (int j = 0; j < BK; ++j)
         if (j < kb) base[j * stride] = x[j];
+    }
     }
     __syncthreads();
     // 3. write the factored diagonal block (one thread, static register

@@ -131,13 +131,99 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Inverse-first node (n <= kNodeGemmMaxN): factor L_i against the identity
+// only, C W = I, so W = C^{-1} comes out of the blocked solve, then every
+// other vector set is one dense GEMM with W (tensor cores for double):
+//     F = R W^T      (rows of the right slot, R loaded row-major)
+//     G = W Lf       (left slot)
+//     y = W y        (factor_and_solve)
+// R, Lf and the first y chunk are loaded together once the factor is done
+// and the three GEMMs run back to back without barriers in between; results
+// go from the accumulators straight to global memory.  Shared layout:
+// S1 (n x ld: A/C, then R), W (n x ld), S2 (n x ld: Lf), Y (n x ldy).
+// INV keeps W^T in the strict upper triangle of L_i.
+// ---------------------------------------------------------------------------
+constexpr int kNodeGemmMaxN = 64;
+__host__ __device__ inline int node_gemm_ldy(int m) { return m > 0 ? even_ld(min_i(m, kMC)) : 0; }
+__host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es) {
+  return 3LL * n * gemm_ld(n, es) + (long long)n * node_gemm_ldy(m);
+}
+
+template <typename T, bool WITH_Y, bool INV>
+__device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level& lv, int b, int t,
+                                               unsigned char* smem_raw) {
+  constexpr int es = sizeof(T);
+  const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
+  const bool right = i + s < p.N, left = t >= 1;
+  const int ld = gemm_ld(n, es);
+  const int ldy = node_gemm_ldy(WITH_Y ? p.m : 0);
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* W = S1 + n * ld;
+  T* S2 = W + n * ld;
+  T* Y = S2 + n * ld;
+  T* Li = p.Lb(b, i);
+  T* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
+  T* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
+  T* yi = WITH_Y ? p.Xb(b, i) : nullptr;
+
+  async_load(S1, ld, Li, n, n, n);
+  if (left) async_load(S2, ld, Lf, n, n, n);   // prefetch: S2 is untouched by the factor
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - r * n;
+    W[r * ld + c] = r == c ? T(1) : T(0);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  cta_chol_solve<T, true>(S1, ld, n, W, ld, n);   // lower(S1) = C, W = C^{-1} (zeros above)
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - r * n;
+    Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : T(0));
+  }
+  __syncthreads();
+  const int mc0 = WITH_Y ? min_i(kMC, p.m) : 0;
+  if (right) async_load(S1, ld, R, n, n, n);
+  if (WITH_Y) async_load(Y, ldy, yi, n, mc0, p.m);
+  cp_async_wait_all();
+  __syncthreads();
+  // F[r][c] = sum_k R[r][k] W[c][k]
+  if (right)
+    cta_gemm<T, false, true>(n, n, n, S1, ld, W, ld, [&](int r, int c, T v) { R[(long long)r * n + c] = v; });
+  // G[r][c] = sum_k W[r][k] Lf[k][c]
+  if (left)
+    cta_gemm<T, false, false>(n, n, n, W, ld, S2, ld, [&](int r, int c, T v) { Lf[(long long)r * n + c] = v; });
+  if (WITH_Y) {
+    for (int c0 = 0; c0 < p.m; c0 += kMC) {
+      const int mc = min_i(kMC, p.m - c0);
+      if (c0 > 0) {
+        __syncthreads();
+        async_load(Y, ldy, yi + c0, n, mc, p.m);
+        cp_async_wait_all();
+        __syncthreads();
+      }
+      cta_gemm<T, false, false>(n, mc, n, W, ld, Y, ldy,
+                                [&](int r, int c, T v) { yi[(long long)r * p.m + c0 + c] = v; });
+    }
+  }
+}
+
+// node body used by the level kernels: inverse-first for small blocks
+__host__ __device__ inline bool node_uses_gemm(int n) { return n <= kNodeGemmMaxN; }
+// dynamic shared memory (elements) of k_node; m_y = right-hand sides solved in the node (0 without y)
+__host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int es) {
+  return node_uses_gemm(n) ? smem_node_gemm_elems(n, m_y, es) : smem_node_elems(n, es);
+}
+
 template <typename T, bool WITH_Y, bool INV = false>
-__global__ void __launch_bounds__(256) k_node(Problem<T> p, Level lv) {
+__global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
   if (!p.active(b)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n));
+  if (node_uses_gemm(p.n))
+    node_gemm_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw);
+  else
+    node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n));
 }
 
 // ---------------------------------------------------------------------------
@@ -221,14 +307,76 @@ __device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv
   }
 }
 
+// Whole-block update for n <= kNodeGemmMaxN: task u-1 < U updates target
+// j = 2su-1 completely (all lower tiles, K = 2n), task U + t-1 forms the whole
+// fill-in block of node t.  One CTA per block keeps every warp busy.
+__host__ __device__ inline int update_blocks(int N, const Level& lv) { return N / (2 * lv.s) + lv.d - 1; }
+__host__ __device__ inline long long smem_update_full_elems(int n, int es) {
+  const long long a = (long long)n * update_ld(2 * n, es);
+  const long long f = 2LL * n * update_ld(n, es);
+  return a > f ? a : f;
+}
+
+template <typename T>
+__device__ __forceinline__ void update_full_body(const Problem<T>& p, const Level& lv, int b, int task,
+                                                 unsigned char* smem_raw) {
+  constexpr int es = sizeof(T);
+  const int n = p.n, N = p.N, s = lv.s;
+  const int U = N / (2 * s);
+  T* Ab = reinterpret_cast<T*>(smem_raw);
+  if (task < U) {
+    const int u = task + 1;
+    const int j = 2 * s * u - 1;
+    const T* F = p.Eb(b, lv.oc + 2 * (u - 1));
+    const bool hasG = j + s < N;
+    const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
+    const int K = hasG ? 2 * n : n;
+    const int lda = update_ld(2 * n, es);
+    // Ab[r][k] = F[r][k], Ab[r][n+k] = G[k][r]
+    async_load(Ab, lda, F, n, n, n);
+    if (hasG) async_load_t(Ab + n, lda, G, n, n, n);
+    cp_async_wait_all();
+    __syncthreads();
+    T* Lj = p.Lb(b, j);
+    cta_gemm<T, false, true, true>(n, n, K, Ab, lda, Ab, lda,
+                                   [&](int r, int c, T v) { Lj[(long long)r * n + c] -= v; });
+  } else {
+    const int t = task - U + 1;
+    const int i = s - 1 + 2 * s * t;
+    if (i + s >= N) return;
+    const T* F = p.Eb(b, lv.oc + 2 * t);
+    const T* G = p.Eb(b, lv.oc + 2 * t - 1);
+    T* X = p.Eb(b, lv.on + t - 1);
+    const int ld = update_ld(n, es);
+    T* Bb = Ab + n * ld;
+    async_load(Ab, ld, F, n, n, n);
+    async_load(Bb, ld, G, n, n, n);
+    cp_async_wait_all();
+    __syncthreads();
+    cta_gemm<T, false, false>(n, n, n, Ab, ld, Bb, ld,
+                              [&](int r, int c, T v) { X[(long long)r * n + c] -= v; });
+  }
+}
+
+__host__ __device__ inline bool update_uses_full(int n) { return n <= kNodeGemmMaxN; }
+__host__ __device__ inline int update_launch_tasks(int n, int N, const Level& lv) {
+  return update_uses_full(n) ? update_blocks(N, lv) : update_tiles(n, N, lv);
+}
+__host__ __device__ inline long long smem_update_launch_elems(int n, int es) {
+  return update_uses_full(n) ? smem_update_full_elems(n, es) : smem_update_elems(n, es);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
-  const int per_b = update_tiles(p.n, p.N, lv);
+  const int per_b = update_launch_tasks(p.n, p.N, lv);
   const int b = blockIdx.x / per_b;
   const int task = blockIdx.x - b * per_b;
   if (!p.active(b)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  update_body<T>(p, lv, b, task, smem_raw);
+  if (update_uses_full(p.n))
+    update_full_body<T>(p, lv, b, task, smem_raw);
+  else
+    update_body<T>(p, lv, b, task, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

@@ -179,7 +179,7 @@ struct RgArgs {
   double tol;
   int max_iter;
   RgQueue q;
-  int vc;                     // vectors per k_node pass
+  int vc;                     // unused (node vectors per pass of the blocked-solve body)
   long long timeout_ns;       // bound of one queue wait
 };
 
@@ -304,22 +304,17 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
     switch (P.kind) {
       case kRgNode: {
         const Problem<T> p = rg_problem(a, I, kPlain ? I.m : 0);
-        node_body<T, kPlain, true>(p, lv, 0, u, smem, a.vc);
+        node_gemm_body<T, kPlain, true>(p, lv, 0, u, smem);
         break;
       }
       case kRgUpd: {
         const Problem<T> p = rg_problem(a, I, kPlain ? I.m : 0);
-        const int nt = ceil_div(I.n, kTile), nlt = nt * (nt + 1) / 2;
         const int U = I.N / (2 * lv.s);
-        for (int lt = 0; lt < nlt; ++lt) {
-          if (lt) __syncthreads();
-          update_body<T>(p, lv, 0, u * nlt + lt, smem);
+        update_full_body<T>(p, lv, 0, u, smem);
+        if (u + 1 <= lv.d - 1) {   // fill-in block of node t = u + 1
+          __syncthreads();
+          update_full_body<T>(p, lv, 0, U + u, smem);
         }
-        if (u + 1 <= lv.d - 1)   // fill-in block of node t = u + 1
-          for (int tt = 0; tt < nt * nt; ++tt) {
-            __syncthreads();
-            update_body<T>(p, lv, 0, U * nlt + u * nt * nt + tt, smem);
-          }
         if constexpr (kPlain) {   // y_j -= F y_{j-s} + G^T y_{j+s} for target j = 2s(u+1) - 1
           __syncthreads();
           fwd_body<T, true, true, false>(p, rg_level(I.N, P.level + 1), 0, u, smem);
