@@ -291,14 +291,19 @@ __device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restric
 // FACTOR = false re-runs the solve with an already factored lower(A) = C.
 // On exit lower(A) = C.  Two barriers per block.
 // ---------------------------------------------------------------------------
-template <typename T, bool FACTOR>
+// IDENTITY: V starts as the n x n identity (nv = n), so it ends as C^{-1}.
+// Rows [K, K+kb) of column c are still zero for c >= K+kb, which leaves those
+// columns out of the item solves and of the trailing update.
+template <typename T, bool FACTOR, bool IDENTITY = false>
 __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
   // diagonal block width: the whole block lives in every thread's registers
   // and is factored redundantly by every thread (work grows as BK^3 x threads)
   constexpr int BK = 8;
+  const int nv_all = nv;
   for (int K = 0; K < n; K += BK) {
     const int kb = min(BK, n - K);
     const int R0 = K + kb, rows = FACTOR ? n - R0 : 0;
+    if (IDENTITY) nv = min(nv_all, R0);
     // 1. diagonal block in registers (identity-padded past kb), only in the
     //    threads that own an item (thread 0 always: it writes the block back)
     T c[BK][BK], rsv[BK];

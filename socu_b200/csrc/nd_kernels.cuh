@@ -175,7 +175,7 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   }
   cp_async_wait_all();
   __syncthreads();
-  cta_chol_solve<T, true>(S1, ld, n, W, ld, n);   // lower(S1) = C, W = C^{-1} (zeros above)
+  cta_chol_solve<T, true, true>(S1, ld, n, W, ld, n);   // lower(S1) = C, W = C^{-1} (zeros above)
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
     Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : T(0));
