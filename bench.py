@@ -300,7 +300,8 @@ def run_ours(args, rank, world, local_rank):
                                    f"({[round(t, 3) for t in cpu_ts]} s)"},
         "e2e": {"value": world / sec_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": sec_e2e * 1e3},
-        "gpu_launches": (mixed.kernel_count + abs(iters) * mixed.round_kernel_count) * args.steps,
+        # graph run: the prologue holds the first round; the WHILE loop runs the others
+        "gpu_launches": (mixed.kernel_count + max(abs(iters) - 1, 0) * mixed.round_kernel_count) * args.steps,
         "clocks": dict(sampler.summary(), window="100 ms samples over all timed regions of this run "
                                                   "(workload, e2e, ragged) and their warm-ups"),
     }

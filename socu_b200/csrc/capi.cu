@@ -305,11 +305,30 @@ RefineArgs refine_args(const double* L, const double* E, const double* b, double
   return a;
 }
 
-// Mixed solve, part 1: state reset, float copies, norms, float factor.
+// One refinement round after a solve that left delta in R32: x += delta,
+// FP64 residual (R32 = r, norms), convergence test.
+int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) {
+  if (count == nullptr) {
+    const long long nvec = (long long)a.B * a.N * a.n * a.m;
+    const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
+    const int nrc = ceil_div(a.n, kResRows);
+    const size_t sres = smem_residual_elems(a.n) * sizeof(double);
+    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+    k_ref_check<<<(a.B + 255) / 256, 256, 0, st>>>(a);
+  } else {
+    *count = 3;
+  }
+  return SOCU_OK;
+}
+
+// Mixed solve, part 1: state reset, float copies, norms, then the first
+// round fused into the float factor: factor_and_solve on R32 = b gives
+// delta = x_1, followed by x += delta, the FP64 residual and the test.
 int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
-  Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
+  Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
@@ -317,34 +336,28 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
     if (e != cudaSuccess) return cuda_status(e);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
     k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+    e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);   // the first test decides
+    if (e != cudaSuccess) return cuda_status(e);
   }
-  long long c = 0;
-  const int s = enqueue<float>(SOCU_OP_FACTOR, pfac, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
-  if (count) *count = 2 + c;
-  (void)d;
+  long long c = 0, cr = 0;
+  int s = enqueue<float>(SOCU_OP_FACTOR_AND_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
+  if (s != SOCU_OK) return s;
+  s = refine_finish_round(a, st, run ? nullptr : &cr);
+  if (count) *count = 2 + c + cr;
   return s;
 }
 
-// Mixed solve, part 2: one refinement round (float solve, x update, FP64
-// residual, convergence test).
+// Mixed solve, part 2: one further refinement round (float solve of R32,
+// x update, FP64 residual, convergence test).
 int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
-  const int nrc = ceil_div(a.n, kResRows);
-  const size_t sres = smem_residual_elems(a.n) * sizeof(double);
-  const long long nvec = (long long)a.B * a.N * a.n * a.m;
-  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
-  const int chk_blocks = (a.B + 255) / 256;
-  long long c = 0;
+  long long c = 0, cr = 0;
   const int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (s != SOCU_OK) return s;
-  if (run) {
-    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
-    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
-    k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
-  }
-  if (count) *count = c + 3;
+  refine_finish_round(a, st, run ? nullptr : &cr);
+  if (count) *count = c + cr;
   return SOCU_OK;
 }
 
@@ -355,12 +368,12 @@ int refine_enqueue(const RefineArgs& a, cudaStream_t st, long long* count) {
   long long cp = 0, ci = 0;
   int s = refine_prologue(a, st, run ? nullptr : &cp);
   if (s != SOCU_OK) return s;
-  for (int it = 0; it < a.max_iter; ++it) {
+  for (int it = 1; it < a.max_iter; ++it) {
     s = refine_iteration(a, st, run ? nullptr : &ci);
     if (s != SOCU_OK) return s;
     if (!run) break;
   }
-  if (count) *count = cp + ci * a.max_iter;
+  if (count) *count = cp + ci * (a.max_iter - 1);
   if (run) return cuda_status(cudaGetLastError());
   return SOCU_OK;
 }
@@ -385,11 +398,19 @@ int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
   cudaGraphNode_t node = nullptr;
   cudaGraph_t bodyg = nullptr;
   if (st == SOCU_OK) {
+    // the handle is created first so that the test after the fused first
+    // round (upstream of the loop) can set it: a solve that converged after
+    // one round never enters the loop
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t* deps = nullptr;
     size_t nd = 0;
     e = cudaStreamGetCaptureInfo(cap, &cs, nullptr, &g, &deps, &nd);
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, g, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      k_ref_decide<<<1, 1, 0, cap>>>(hnd, a.any_active);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cap, &cs, nullptr, &g, &deps, &nd);
     cudaGraphNodeParams prm = {};
     prm.type = cudaGraphNodeTypeConditional;
     prm.conditional.handle = hnd;
@@ -557,7 +578,7 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
     for (int ph = 0; ph < phases; ++ph) cap += rg_chunks(rg_phase(I, mode, ph));
     maxn = std::max(maxn, I.n);
     maxm = std::max(maxm, I.m);
-    maxnv = std::max(maxnv, 3 * I.n + (r->refine ? 0 : I.m));
+    maxnv = std::max(maxnv, 3 * I.n + I.m);
   }
   // first-phase chunks, largest instances first
   std::vector<int> order(r->inst.size());
@@ -574,7 +595,7 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
   // shared memory: the largest body at the largest block size (n <= 64: the
   // inverse-first node body)
   r->vc = maxnv;
-  size_t smem = (size_t)smem_node_gemm_elems(maxn, r->refine ? 0 : maxm, es) * es;
+  size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es) * es;
   smem = std::max(smem, (size_t)smem_update_full_elems(maxn, es) * es);
   smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
   if (r->refine) smem = std::max(smem, (size_t)smem_residual_elems(maxn) * sizeof(double));
@@ -807,20 +828,21 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   }
   const Dims d{a.B, a.N, a.n, a.m, a.S};
   const Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
-  const Problem<float> pfac = make_problem<float>(a.L32, a.E32, nullptr, a.active, Dims{a.B, a.N, a.n, 0, a.S});
   const int n = a.n, nth = threads_for(n);
-  const size_t sd = smem_node_launch_elems(n, 0, sizeof(float)) * sizeof(float);
+  const size_t sd = smem_node_launch_elems(n, a.m, sizeof(float)) * sizeof(float);
   const size_t su = smem_update_launch_elems(n, sizeof(float)) * sizeof(float);
   const bool res = (long long)smem_sweep_res_elems(n, a.m) * (long long)sizeof(float) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, a.m) : smem_sweep_elems(n, a.m)) * sizeof(float);
   const size_t sres = smem_residual_elems(n) * sizeof(double);
   const bool inv = use_inverse<float>(n, a.m);
-  auto node = inv ? k_node<float, false, true> : k_node<float, false, false>;
+  auto node = inv ? k_node<float, true, true> : k_node<float, true, false>;
   auto fwd = res ? (inv ? k_fwd<float, true, false, true> : k_fwd<float, true>) : k_fwd<float, false>;
+  auto pull = res ? k_fwd<float, true, true> : k_fwd<float, false, true>;
   auto bwd = res ? (inv ? k_bwd<float, true, true> : k_bwd<float, true>) : k_bwd<float, false>;
   cudaError_t e = noalloc_smem(node, sd);
   if (e == cudaSuccess) e = noalloc_smem(k_update<float>, su);
   if (e == cudaSuccess) e = noalloc_smem(fwd, ss);
+  if (e == cudaSuccess) e = noalloc_smem(pull, ss);
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
   if (e != cudaSuccess) return cuda_status(e);
@@ -833,16 +855,19 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e != cudaSuccess) return cuda_status(e);
   k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
   k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+  // first round fused into the float factor: factor_and_solve of R32 = b
   for (int l = 0; l < K; ++l) {
-    node<<<(unsigned)((long long)a.B * lv[l].d), nth, sd, st>>>(pfac, lv[l]);
+    node<<<(unsigned)((long long)a.B * lv[l].d), nth, sd, st>>>(pf, lv[l]);
     if (l + 1 < K) {
       const long long blocks = (long long)a.B * update_launch_tasks(n, a.N, lv[l]);
-      if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pfac, lv[l]);
+      if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pf, lv[l]);
+      pull<<<(unsigned)((long long)a.B * (a.N / lv[l + 1].s)), nth, ss, st>>>(pf, lv[l + 1]);
     }
   }
   for (int it = 0; it < a.max_iter; ++it) {
-    for (int l = 0; l < K; ++l)
-      fwd<<<(unsigned)((long long)a.B * (l == 0 ? lv[l].d : a.N / lv[l].s)), nth, ss, st>>>(pf, lv[l]);
+    if (it > 0)
+      for (int l = 0; l < K; ++l)
+        fwd<<<(unsigned)((long long)a.B * (l == 0 ? lv[l].d : a.N / lv[l].s)), nth, ss, st>>>(pf, lv[l]);
     for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
     k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
@@ -1091,11 +1116,12 @@ int socu_refine_launch_create(socu_launch_t* out, const double* L, const double*
       delete h;
       return st;
     }
-    // kernels per run: prologue + one round (+ loop control) per round executed
+    // kernels per run: prologue with the first round and the loop test, then
+    // one round (+ loop control) per further round executed
     long long cp = 0, ci = 0;
     refine_prologue(h->ra, nullptr, &cp);
     refine_iteration(h->ra, nullptr, &ci);
-    h->kernels = cp;
+    h->kernels = cp + 1;
     h->round_kernels = ci + 1;
   }
   (void)stream;

@@ -11,9 +11,10 @@
 //   plain factor_and_solve (T = float or double), K separator levels:
 //     NODE 0, UPD 0, NODE 1, UPD 1, ..., NODE K-1, BWD K-1, ..., BWD 0
 //   mixed refinement (T = float factor of an FP64 problem):
-//     INIT, NODE 0, UPD 0, ..., NODE K-1, then per round
-//     FWD 0..K-1, BWD K-1..0, XUPD (x += delta), RES (FP64 residual and eta)
-//     until eta <= tol, max_iter rounds, or a non-finite eta.
+//     INIT, then the plain phases on the float copy with y = b (the first
+//     round fused into the factor), XUPD (x += delta), RES (FP64 residual and
+//     eta); every further round is FWD 0..K-1, BWD K-1..0, XUPD, RES, until
+//     eta <= tol, max_iter rounds, or a non-finite eta.
 //
 // NODE/UPD/FWD/BWD/RES run the same device bodies as the per-level kernels of
 // the uniform batch (nd_kernels.cuh, refine.cuh), so each output block has one
@@ -89,7 +90,7 @@ __host__ __device__ inline int rg_res_panels(int n) { return (n + kResRows - 1) 
 // Phases of the plain path; the refinement path is unbounded (decided on the device).
 __host__ __device__ inline int rg_plain_phases(int K) { return 3 * K - 1; }
 // Phases of the refinement path with `rounds` refinement rounds.
-__host__ __device__ inline int rg_refine_phases(int K, int rounds) { return 2 * K + rounds * (2 * K + 2); }
+__host__ __device__ inline int rg_refine_phases(int K, int rounds) { return 3 * K + 2 + (rounds - 1) * (2 * K + 2); }
 
 __host__ __device__ inline RgPhase rg_phase(const RgInst& I, int mode, int ph) {
   const int K = I.K;
@@ -119,13 +120,15 @@ __host__ __device__ inline RgPhase rg_phase(const RgInst& I, int mode, int ph) {
     return r;
   }
   f -= 2 * K - 1;
-  if (mode == kRgPlain) {
+  if (mode == kRgPlain || f < K) {
     r.kind = kRgBwd;
     r.level = K - 1 - f;
     r.units = rg_level(I.N, r.level).d;
     return r;
   }
-  const int q = f % (2 * K + 2);
+  // refinement: XUPD and RES of the first round, then whole rounds
+  f -= K;
+  const int q = f < 2 ? 2 * K + f : (f - 2) % (2 * K + 2);
   if (q < K) {
     r.kind = kRgFwd;
     r.level = q;
@@ -303,22 +306,21 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
     if (u > u0) __syncthreads();
     switch (P.kind) {
       case kRgNode: {
-        const Problem<T> p = rg_problem(a, I, kPlain ? I.m : 0);
-        node_gemm_body<T, kPlain, true>(p, lv, 0, u, smem);
+        const Problem<T> p = rg_problem(a, I, I.m);
+        node_gemm_body<T, true, true>(p, lv, 0, u, smem);
         break;
       }
       case kRgUpd: {
-        const Problem<T> p = rg_problem(a, I, kPlain ? I.m : 0);
+        const Problem<T> p = rg_problem(a, I, I.m);
         const int U = I.N / (2 * lv.s);
         update_full_body<T>(p, lv, 0, u, smem);
         if (u + 1 <= lv.d - 1) {   // fill-in block of node t = u + 1
           __syncthreads();
           update_full_body<T>(p, lv, 0, U + u, smem);
         }
-        if constexpr (kPlain) {   // y_j -= F y_{j-s} + G^T y_{j+s} for target j = 2s(u+1) - 1
-          __syncthreads();
-          fwd_body<T, true, true, false>(p, rg_level(I.N, P.level + 1), 0, u, smem);
-        }
+        // y_j -= F y_{j-s} + G^T y_{j+s} for target j = 2s(u+1) - 1
+        __syncthreads();
+        fwd_body<T, true, true, false>(p, rg_level(I.N, P.level + 1), 0, u, smem);
         break;
       }
       case kRgBwd: {
