@@ -39,6 +39,11 @@ def storage_len(N):
 
 
 RAGGED_COUNT, RAGGED_SEED = 4096, 0
+# DRAM bytes (read + write) per k_bwd<float, resident, inverse> launch, averaged
+# over one backward sweep of this workload, from the ncu capture summarised in
+# profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md
+TRAFFIC_BYTES = 4999401
+TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md"
 RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
                    "instance i seeded with 0 + i, one persistent launch per solve")
 
@@ -175,7 +180,8 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from socu_b200.block_tridiag_solver import create_cholesky_factor_and_solve_launch, create_cholesky_factor_launch
+    from socu_b200.block_tridiag_solver import (create_cholesky_backward_substitution_launch,
+                                                create_cholesky_factor_and_solve_launch, create_cholesky_factor_launch)
     from socu_b200.mixed import backward_error, create_cholesky_refined_solve_launch
 
     dev = torch.device("cuda", local_rank)
@@ -191,13 +197,27 @@ def run_ours(args, rank, world, local_rank):
 
     # mixed + refinement (headline), inputs read-only
     mixed = create_cholesky_refined_solve_launch(L0, E0, b0, x, tol=TOL, max_iter=MAX_ITER, use_cuda_graph=True)
+    if args.profile:
+        # profiler runs: ncu does not report kernels inside the conditional WHILE
+        # graph node, so run the same kernels without a graph, with max_iter set to
+        # the rounds the graph run needs (the graph only adds its loop-control kernels)
+        mixed()
+        torch.cuda.synchronize(dev)
+        rounds = max(1, int(mixed.iterations.abs().max()))
+        mixed = create_cholesky_refined_solve_launch(L0, E0, b0, x, tol=TOL, max_iter=rounds, use_cuda_graph=False)
     # plain FP64 factor_and_solve on working copies (in place)
     Lw, Ew, xw = L0.clone(), E0.clone(), b0.clone()
     plain = create_cholesky_factor_and_solve_launch(Lw, Ew, xw, use_cuda_graph=True)
-    # float factor alone, for the dominant-phase roofline
+    # the dominant kernel of the mixed solve: the float backward sweep on a
+    # factor that carries its diagonal inverses (k_bwd<float, resident, inverse>),
+    # one launch per level, timed as whole graph-launched sweeps
     L32, E32 = L0.float(), E0.float()
-    L32w, E32w = L32.clone(), E32.clone()
-    fac32 = create_cholesky_factor_launch(L32w, E32w, dtype=torch.float32, use_cuda_graph=True)
+    create_cholesky_factor_launch(L32, E32, dtype=torch.float32, keep_inverse=True)()
+    b32 = b0.float()
+    x32 = b32.clone()
+    fac32 = create_cholesky_backward_substitution_launch(L32, E32, x32, dtype=torch.float32, use_cuda_graph=True,
+                                                         factor_has_inverse=True)
+    sweep_launches = fac32.kernel_count
 
     def time_steps(fn, reset, k):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
@@ -214,7 +234,7 @@ def run_ours(args, rank, world, local_rank):
         Lw.copy_(L0); Ew.copy_(E0); xw.copy_(b0)
 
     def reset_fac():
-        L32w.copy_(L32); E32w.copy_(E32)
+        x32.copy_(b32)
 
     nothing = lambda: None
     # clocks are sampled over the whole measurement window (every timed region
@@ -261,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
         return float(v)
 
     sec_mixed, sec_plain, sec_fac, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_fac), agg(t_e2e)
-    del e2e_run, Ld, Ed, bd, xd, Lw, Ew, xw, L32, E32, L32w, E32w
+    del e2e_run, Ld, Ed, bd, xd, Lw, Ew, xw, L32, E32, x32, b32
     torch.cuda.empty_cache()
     rg = bench_ragged(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
     barrier()
@@ -270,7 +290,12 @@ def run_ours(args, rank, world, local_rank):
         return
     n, N, m = BLOCK, N_BLOCKS, NRHS
     S = storage_len(N)
-    fac_bytes = 2.0 * (N + S) * n * n * 4   # read + write the float L and E once
+    # algorithmic bytes of one backward sweep: every diagonal block (with its
+    # inverse) and every coupling slot read once, x read three times and
+    # written once per node, 4-byte floats; per launch = sweep / launches
+    sweep_bytes = ((N + S) * n * n + 4.0 * N * n * m) * 4
+    fac_bytes = sweep_bytes / sweep_launches
+    sec_fac = sec_fac / sweep_launches
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -291,10 +316,12 @@ def run_ours(args, rank, world, local_rank):
         "mixed_over_fp64": sec_plain / sec_mixed,
         "backward_error": {"max": eta_dev, "recomputed": eta_check, "iterations": iters},
         "factor_flops_fp": algorithmic_factor_flops(N, n),
-        "roofline": {"kernel": "float factor (k_node + k_update per level)", "bound": "hbm",
+        "roofline": {"kernel": "k_bwd<float, resident, inverse> (backward sweep of the mixed solve; "
+                               f"{sweep_launches} launches per sweep, averaged)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "peak_source": peak_src, "traffic": None,
-                     "algorithmic_bytes": fac_bytes, "ms_per_launch": sec_fac * 1e3},
+                     "peak_source": peak_src, "traffic": TRAFFIC_BYTES,
+                     "algorithmic_bytes": fac_bytes, "ms_per_launch": sec_fac * 1e3,
+                     "traffic_source": TRAFFIC_NOTE},
         "cpu_baseline": {"value": cpu_v, "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": "one FP64 factor_and_solve of the workload system, median of 2 "
                                    f"({[round(t, 3) for t in cpu_ts]} s)"},
@@ -365,6 +392,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch measurement")
+    ap.add_argument("--profile", action="store_true",
+                    help="for profiler runs only: the mixed solve runs without its CUDA graph")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -37,12 +37,23 @@ extern "C" {
 
 typedef enum socu_dtype { SOCU_FLOAT32 = 0, SOCU_FLOAT64 = 1 } socu_dtype;
 
+/* Operations 0-4 are the reference's five launches.  5-8 are an extension
+ * (no counterpart in the reference) for factor reuse: SOCU_OP_FACTOR_INV
+ * factors like SOCU_OP_FACTOR and also keeps W_i^T = C_i^{-T} in the strict
+ * upper triangle of each L_i (as SOCU_OP_FACTOR_AND_SOLVE does); the *_INV
+ * sweeps require such a factor and apply W_i as a matrix-vector product
+ * instead of a triangular solve.  Blocks with n <= 64 only (larger n:
+ * SOCU_ERR_UNSUPPORTED). */
 typedef enum socu_op {
   SOCU_OP_FACTOR = 0,
   SOCU_OP_FACTOR_AND_SOLVE = 1,
   SOCU_OP_FORWARD_SUBSTITUTION = 2,
   SOCU_OP_BACKWARD_SUBSTITUTION = 3,
-  SOCU_OP_SOLVE = 4
+  SOCU_OP_SOLVE = 4,
+  SOCU_OP_FACTOR_INV = 5,
+  SOCU_OP_FORWARD_INV = 6,
+  SOCU_OP_BACKWARD_INV = 7,
+  SOCU_OP_SOLVE_INV = 8
 } socu_op;
 
 /* Library version string. */
@@ -89,6 +100,10 @@ int socu_cholesky_backward_substitution(socu_dtype dtype, const void* L, const v
 int socu_cholesky_solve(socu_dtype dtype, const void* L, const void* E, void* x,
                         const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n,
                         int64_t n_rhs, void* stream);
+
+/* Any socu_op (0-8) as a direct call; x is ignored for the two factor ops. */
+int socu_cholesky_run(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask, int64_t batch,
+                      int64_t horizon, int64_t n, int64_t n_rhs, void* stream);
 
 /* Recorded launches bound to fixed buffers, optionally captured once into a
  * CUDA graph at creation (the recorded launches + create_cuda_graph_callback

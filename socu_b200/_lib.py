@@ -31,6 +31,10 @@ OP_FACTOR_AND_SOLVE = 1
 OP_FORWARD = 2
 OP_BACKWARD = 3
 OP_SOLVE = 4
+OP_FACTOR_INV = 5
+OP_FORWARD_INV = 6
+OP_BACKWARD_INV = 7
+OP_SOLVE_INV = 8
 
 _lock = threading.Lock()
 _lib = None
@@ -52,6 +56,7 @@ _SIGNATURES = {
     "socu_cholesky_forward_substitution": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
     "socu_cholesky_backward_substitution": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
     "socu_cholesky_solve": (_int, [_int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
+    "socu_cholesky_run": (_int, [_int, _int, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _vp]),
     "socu_launch_create": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p,
                                   _i64, _i64, _i64, _i64, _int, _vp]),
     "socu_launch_run": (_int, [_vp, _vp]),

@@ -220,9 +220,13 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x):
 
 def create_cholesky_factor_launch(L, E, mask=None, block_dim=None, block_size=None,
                                   dtype=torch.float64, device=None, stream=None,
-                                  use_cuda_graph=False):
-    """In-place ND Cholesky factor of (L, E); returns a zero-argument callable."""
-    return _create(_lib.OP_FACTOR, L, E, None, mask, dtype, device, stream, use_cuda_graph, False)
+                                  use_cuda_graph=False, *, keep_inverse=False):
+    """In-place ND Cholesky factor of (L, E); returns a zero-argument callable.
+
+    keep_inverse (extension, n <= 64): also store W_i^T = C_i^{-T} in the strict
+    upper triangle of every L_i, for the ``factor_has_inverse`` sweeps."""
+    op = _lib.OP_FACTOR_INV if keep_inverse else _lib.OP_FACTOR
+    return _create(op, L, E, None, mask, dtype, device, stream, use_cuda_graph, False)
 
 
 def create_cholesky_factor_and_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
@@ -234,20 +238,35 @@ def create_cholesky_factor_and_solve_launch(L, E, x, mask=None, block_dim=None, 
 
 def create_cholesky_forward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
                                                 dtype=torch.float64, device=None, stream=None,
-                                                use_cuda_graph=False):
-    """Forward sweep on a stored factor; x: b in, y out."""
-    return _create(_lib.OP_FORWARD, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+                                                use_cuda_graph=False, *, factor_has_inverse=False):
+    """Forward sweep on a stored factor; x: b in, y out.
+
+    factor_has_inverse (extension, n <= 64): the factor carries W_i^T in its
+    upper triangles (factor_and_solve, or factor with keep_inverse=True); the
+    sweep then multiplies by W_i instead of solving with C_i."""
+    op = _lib.OP_FORWARD_INV if factor_has_inverse else _lib.OP_FORWARD
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
 
 
 def create_cholesky_backward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
                                                  dtype=torch.float64, device=None, stream=None,
-                                                 use_cuda_graph=False):
-    """Backward sweep on a stored factor; x: y in, solution out."""
-    return _create(_lib.OP_BACKWARD, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+                                                 use_cuda_graph=False, *, factor_has_inverse=False):
+    """Backward sweep on a stored factor; x: y in, solution out.
+
+    factor_has_inverse (extension, n <= 64): the factor carries W_i^T in its
+    upper triangles (factor_and_solve, or factor with keep_inverse=True); the
+    sweep then multiplies by W_i instead of solving with C_i."""
+    op = _lib.OP_BACKWARD_INV if factor_has_inverse else _lib.OP_BACKWARD
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
 
 
 def create_cholesky_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
                                  dtype=torch.float64, device=None, stream=None,
-                                 use_cuda_graph=False):
-    """Forward then backward sweep on a stored factor; x: b in, solution out."""
-    return _create(_lib.OP_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+                                 use_cuda_graph=False, *, factor_has_inverse=False):
+    """Forward then backward sweep on a stored factor; x: b in, solution out.
+
+    factor_has_inverse (extension, n <= 64): the factor carries W_i^T in its
+    upper triangles (factor_and_solve, or factor with keep_inverse=True); the
+    sweep then multiplies by W_i instead of solving with C_i."""
+    op = _lib.OP_SOLVE_INV if factor_has_inverse else _lib.OP_SOLVE
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)

@@ -197,10 +197,24 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   return SOCU_OK;
 }
 
+// The *_INV extension ops run the base op on a factor that carries W^T.
+socu_op base_op(socu_op op, bool* inv) {
+  *inv = (int)op >= (int)SOCU_OP_FACTOR_INV;
+  switch (op) {
+    case SOCU_OP_FACTOR_INV: return SOCU_OP_FACTOR;
+    case SOCU_OP_FORWARD_INV: return SOCU_OP_FORWARD_SUBSTITUTION;
+    case SOCU_OP_BACKWARD_INV: return SOCU_OP_BACKWARD_SUBSTITUTION;
+    case SOCU_OP_SOLVE_INV: return SOCU_OP_SOLVE;
+    default: return op;
+  }
+}
+
 int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const void* x,
              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, Dims* d) {
   if (dtype != SOCU_FLOAT32 && dtype != SOCU_FLOAT64) return SOCU_ERR_INVALID_ARGUMENT;
-  if ((int)op < 0 || (int)op > 4) return SOCU_ERR_INVALID_ARGUMENT;
+  if ((int)op < 0 || (int)op > 8) return SOCU_ERR_INVALID_ARGUMENT;
+  bool inv_op = false;
+  op = base_op(op, &inv_op);
   if (batch < 0 || horizon <= 0 || n <= 0) return SOCU_ERR_INVALID_ARGUMENT;
   const bool needs_x = op != SOCU_OP_FACTOR;
   if (needs_x && n_rhs <= 0) return SOCU_ERR_INVALID_ARGUMENT;
@@ -213,6 +227,11 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
     if (needs_x && x == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
   }
   if ((int64_t)n > socu_max_block_size(dtype, needs_x ? n_rhs : 0)) return SOCU_ERR_UNSUPPORTED;
+  if (inv_op) {
+    const int mm = needs_x ? (int)n_rhs : 1;
+    const bool ok = dtype == SOCU_FLOAT64 ? use_inverse<double>((int)n, mm) : use_inverse<float>((int)n, mm);
+    if (!ok) return SOCU_ERR_UNSUPPORTED;
+  }
   d->B = (int)batch;
   d->N = (int)horizon;
   d->n = (int)n;
@@ -241,8 +260,11 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
     if (e != cudaSuccess) return cuda_status(e);
   }
   // factor_and_solve keeps the diagonal inverses in the (unspecified) upper
-  // triangles of L and uses them for its own backward sweep
-  const bool inv = op == SOCU_OP_FACTOR_AND_SOLVE;
+  // triangles of L and uses them for its own backward sweep; the *_INV ops
+  // keep or use them on request
+  bool inv = false;
+  op = base_op(op, &inv);
+  inv = inv || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (dtype == SOCU_FLOAT64)
     return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv);
   return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv);
@@ -960,6 +982,11 @@ int socu_cholesky_solve(socu_dtype dtype, const void* L, const void* E, void* x,
                         int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream) {
   return dispatch(SOCU_OP_SOLVE, dtype, const_cast<void*>(L), const_cast<void*>(E), x, mask, batch,
                   horizon, n, n_rhs, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int socu_cholesky_run(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask, int64_t batch,
+                      int64_t horizon, int64_t n, int64_t n_rhs, void* stream) {
+  return dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, static_cast<cudaStream_t>(stream), nullptr);
 }
 
 int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
