@@ -334,9 +334,13 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     const long long nvec = (long long)a.B * a.N * a.n * a.m;
     const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
     const int nrc = ceil_div(a.n, kResRows);
-    const size_t sres = smem_residual_elems(a.n) * sizeof(double);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
-    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+    if (residual_uses_rows(a.n))
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, smem_residual_rows_elems(a.n) * sizeof(double),
+                              st>>>(a);
+    else
+      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
+                         st>>>(a);
     k_ref_check<<<(a.B + 255) / 256, 256, 0, st>>>(a);
   } else {
     *count = 3;
@@ -354,10 +358,17 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
+    const size_t srow = smem_residual_rows_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
+    if (e == cudaSuccess) e = prepare(k_residual_rows<true>, srow);
+    if (e == cudaSuccess) e = prepare(k_ref_init_rows, srow);
     if (e != cudaSuccess) return cuda_status(e);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
-    k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+    const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
+    if (residual_uses_rows(a.n))
+      k_ref_init_rows<<<init_blocks, 256, srow, st>>>(a);
+    else
+      k_ref_init<<<init_blocks, 256, 0, st>>>(a);
     e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);   // the first test decides
     if (e != cudaSuccess) return cuda_status(e);
   }
@@ -620,7 +631,7 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
   size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es) * es;
   smem = std::max(smem, (size_t)smem_update_full_elems(maxn, es) * es);
   smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
-  if (r->refine) smem = std::max(smem, (size_t)smem_residual_elems(maxn) * sizeof(double));
+  if (r->refine) smem = std::max(smem, (size_t)smem_residual_rows_elems(maxn) * sizeof(double));
   if ((long long)smem > (long long)max_smem_optin()) return SOCU_ERR_UNSUPPORTED;
   r->smem = smem;
   cudaError_t e = cudaGetDevice(&r->device);
@@ -867,6 +878,9 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e == cudaSuccess) e = noalloc_smem(pull, ss);
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
+  const size_t srow = smem_residual_rows_elems(n) * sizeof(double);
+  if (e == cudaSuccess) e = noalloc_smem(k_residual_rows<true>, srow);
+  if (e == cudaSuccess) e = noalloc_smem(k_ref_init_rows, srow);
   if (e != cudaSuccess) return cuda_status(e);
   (void)0;
   const int nrc = ceil_div(n, kResRows);
@@ -876,7 +890,12 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_status(e);
   k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
-  k_ref_init<<<(unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S)), 256, 0, st>>>(a);
+  const bool rows = residual_uses_rows(n);
+  const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
+  if (rows)
+    k_ref_init_rows<<<init_blocks, 256, srow, st>>>(a);
+  else
+    k_ref_init<<<init_blocks, 256, 0, st>>>(a);
   // first round fused into the float factor: factor_and_solve of R32 = b
   for (int l = 0; l < K; ++l) {
     node<<<(unsigned)((long long)a.B * lv[l].d), nth, sd, st>>>(pf, lv[l]);
@@ -892,7 +911,10 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
         fwd<<<(unsigned)((long long)a.B * (l == 0 ? lv[l].d : a.N / lv[l].s)), nth, ss, st>>>(pf, lv[l]);
     for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
-    k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
+    if (rows)
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, srow, st>>>(a);
+    else
+      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
     k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
   }
   return cuda_status(cudaGetLastError());
@@ -1097,10 +1119,17 @@ int socu_block_tridiag_residual(const double* L, const double* E, const double* 
   a.L = L; a.E = E; a.b = b; a.x = const_cast<double*>(x); a.rout = r;
   a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
   const size_t sres = smem_residual_elems(d.n) * sizeof(double);
-  e = prepare(k_residual<false>, sres);
-  if (e != cudaSuccess) return cuda_status(e);
-  const int nrc = ceil_div(d.n, kResRows);
-  k_residual<false><<<(unsigned)((long long)d.B * d.N * nrc), 256, sres, static_cast<cudaStream_t>(stream)>>>(a);
+  const size_t srow = smem_residual_rows_elems(d.n) * sizeof(double);
+  if (residual_uses_rows(d.n)) {
+    e = prepare(k_residual_rows<false>, srow);
+    if (e != cudaSuccess) return cuda_status(e);
+    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), 256, srow, static_cast<cudaStream_t>(stream)>>>(a);
+  } else {
+    e = prepare(k_residual<false>, sres);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int nrc = ceil_div(d.n, kResRows);
+    k_residual<false><<<(unsigned)((long long)d.B * d.N * nrc), 256, sres, static_cast<cudaStream_t>(stream)>>>(a);
+  }
   return cuda_status(cudaGetLastError());
 }
 

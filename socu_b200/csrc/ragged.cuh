@@ -85,8 +85,6 @@ __host__ __device__ inline Level rg_level(int N, int l) {
   return lv;
 }
 
-__host__ __device__ inline int rg_res_panels(int n) { return (n + kResRows - 1) / kResRows; }
-
 // Phases of the plain path; the refinement path is unbounded (decided on the device).
 __host__ __device__ inline int rg_plain_phases(int K) { return 3 * K - 1; }
 // Phases of the refinement path with `rounds` refinement rounds.
@@ -145,7 +143,7 @@ __host__ __device__ inline RgPhase rg_phase(const RgInst& I, int mode, int ph) {
   } else {
     r.kind = kRgRes;
     r.level = 0;
-    r.units = I.N * rg_res_panels(I.n);
+    r.units = I.N;   // block rows (n <= 64: one CTA pass per row)
   }
   return r;
 }
@@ -336,13 +334,12 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
         break;
       }
       case kRgInit: {
-        if constexpr (!kPlain) ref_init_body(rg_refine_args(a, I, ii), 0, u);
+        if constexpr (!kPlain) ref_init_rows_body(rg_refine_args(a, I, ii), 0, u, smem);
         break;
       }
       case kRgRes: {
         if constexpr (!kPlain) {
-          const int nrc = rg_res_panels(I.n);
-          residual_body<true>(rg_refine_args(a, I, ii), 0, u / nrc, (u % nrc) * kResRows, smem);
+          residual_rows_body<true>(rg_refine_args(a, I, ii), 0, u, smem);
         }
         break;
       }

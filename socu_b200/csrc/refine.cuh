@@ -233,6 +233,181 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
   residual_body<REFINE>(a, bi, i, (rem - i * nrc) * kResRows, smem_raw);
 }
 
+// ---------------------------------------------------------------------------
+// Block-row kernels for n <= kResRowMaxN: one CTA per block row i stages the
+// three blocks of that row, L_i, E_{i-1} and E_i, in shared memory with
+// coalesced loads (missing neighbours as zeros), so every element of L and E
+// is read from HBM once per row that needs it and never column-wise.
+// Shared: Ls, Em, Ep (n x (n+1) each), X0, X1, X2 (n x (kResRowCols+1)).
+// ---------------------------------------------------------------------------
+constexpr int kResRowMaxN = 64;
+constexpr int kResRowCols = 8;
+__host__ __device__ inline long long smem_residual_rows_elems(int n) {
+  return 3LL * n * (n + 1) + 3LL * n * (kResRowCols + 1);
+}
+__host__ __device__ inline bool residual_uses_rows(int n) { return n <= kResRowMaxN; }
+
+__device__ __forceinline__ void stage_block_row(const RefineArgs& a, int bi, int i, double* Ls, double* Em,
+                                                double* Ep) {
+  const int n = a.n, N = a.N, ld = n + 1;
+  const long long nn = (long long)n * n;
+  async_load(Ls, ld, a.L + ((long long)bi * N + i) * nn, n, n, n);
+  if (i > 0) {
+    async_load(Em, ld, a.E + ((long long)bi * a.S + i - 1) * nn, n, n, n);
+  } else {
+    for (int e = threadIdx.x; e < n * ld; e += blockDim.x) Em[e] = 0.0;
+  }
+  if (i < N - 1) {
+    async_load(Ep, ld, a.E + ((long long)bi * a.S + i) * nn, n, n, n);
+  } else {
+    for (int e = threadIdx.x; e < n * ld; e += blockDim.x) Ep[e] = 0.0;
+  }
+}
+
+// r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block row.
+template <bool REFINE>
+__device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
+  const int n = a.n, m = a.m, N = a.N, ld = n + 1, ldx = kResRowCols + 1;
+  double* Ls = reinterpret_cast<double*>(smem_raw);
+  double* Em = Ls + n * ld;
+  double* Ep = Em + n * ld;
+  double* X0 = Ep + n * ld;
+  double* X1 = X0 + n * ldx;
+  double* X2 = X1 + n * ldx;
+  __shared__ double red[32];
+  stage_block_row(a, bi, i, Ls, Em, Ep);
+  const long long vi = ((long long)bi * N + i) * n * m;
+  double rmax = 0.0, xmax = 0.0;
+  for (int c0 = 0; c0 < m; c0 += kResRowCols) {
+    const int mc = min(kResRowCols, m - c0);
+    __syncthreads();
+    async_load(X1, ldx, a.x + vi + c0, n, mc, m);
+    if (i > 0) {
+      async_load(X0, ldx, a.x + vi - (long long)n * m + c0, n, mc, m);
+    } else {
+      for (int e = threadIdx.x; e < n * ldx; e += blockDim.x) X0[e] = 0.0;
+    }
+    if (i < N - 1) {
+      async_load(X2, ldx, a.x + vi + (long long)n * m + c0, n, mc, m);
+    } else {
+      for (int e = threadIdx.x; e < n * ldx; e += blockDim.x) X2[e] = 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
+      const int r = o / mc, c = o - r * mc;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, s5 = 0.0;
+      int k = 0;
+      for (; k + 1 < n; k += 2) {
+        const double d0 = k <= r ? Ls[r * ld + k] : Ls[k * ld + r];
+        const double d1 = k + 1 <= r ? Ls[r * ld + k + 1] : Ls[(k + 1) * ld + r];
+        s0 = fma(d0, X1[k * ldx + c], s0);
+        s3 = fma(d1, X1[(k + 1) * ldx + c], s3);
+        s1 = fma(Em[r * ld + k], X0[k * ldx + c], s1);
+        s4 = fma(Em[r * ld + k + 1], X0[(k + 1) * ldx + c], s4);
+        s2 = fma(Ep[k * ld + r], X2[k * ldx + c], s2);
+        s5 = fma(Ep[(k + 1) * ld + r], X2[(k + 1) * ldx + c], s5);
+      }
+      if (k < n) {
+        const double d0 = k <= r ? Ls[r * ld + k] : Ls[k * ld + r];
+        s0 = fma(d0, X1[k * ldx + c], s0);
+        s1 = fma(Em[r * ld + k], X0[k * ldx + c], s1);
+        s2 = fma(Ep[k * ld + r], X2[k * ldx + c], s2);
+      }
+      const long long e = vi + (long long)r * m + c0 + c;
+      const double res = a.b[e] - (((s0 + s3) + (s1 + s4)) + (s2 + s5));
+      if (REFINE) {
+        a.R32[e] = (float)res;
+        const double xv = X1[r * ldx + c];
+        rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
+        xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
+      } else {
+        a.rout[e] = res;
+      }
+    }
+  }
+  if (REFINE) {
+    const double rm = block_max(rmax, red);
+    const double xm = block_max(xmax, red);
+    if (threadIdx.x == 0) {
+      atomic_max_pos(&a.st[bi].rnorm, rm);
+      atomic_max_pos(&a.st[bi].xnorm, xm);
+    }
+  }
+}
+
+template <bool REFINE>
+__global__ void __launch_bounds__(256) k_residual_rows(RefineArgs a) {
+  const int bi = blockIdx.x / a.N;
+  const int i = blockIdx.x - bi * a.N;
+  if (REFINE && !a.active[bi]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  residual_rows_body<REFINE>(a, bi, i, smem_raw);
+}
+
+// Refinement set-up for block row i (if i < N) and storage slot i (if i < S):
+// float copies of L_i and slot i, R32 = b_i, x_i = 0, ||b||_inf and the row
+// sums of |Psi| over block row i, all from shared memory.
+__device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
+  __shared__ double red[32];
+  const int n = a.n, m = a.m, N = a.N, ld = n + 1;
+  const long long nn = (long long)n * n;
+  if (i >= N) {   // storage tail: zero slots only
+    if (i < a.S) {
+      float* E32 = a.E32 + ((long long)bi * a.S + i) * nn;
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) E32[e] = 0.0f;
+    }
+    return;
+  }
+  double* Ls = reinterpret_cast<double*>(smem_raw);
+  double* Em = Ls + n * ld;
+  double* Ep = Em + n * ld;
+  stage_block_row(a, bi, i, Ls, Em, Ep);
+  const long long vo = ((long long)bi * N + i) * n * m;
+  double bmax = 0.0;
+  for (int e = threadIdx.x; e < n * m; e += blockDim.x) {
+    const double v = a.b[vo + e];
+    a.R32[vo + e] = (float)v;
+    a.x[vo + e] = 0.0;
+    bmax = fmax(bmax, fabs(v));
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  float* L32 = a.L32 + ((long long)bi * N + i) * nn;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) L32[e] = (float)Ls[(e / n) * ld + e % n];
+  if (i < a.S) {
+    float* E32 = a.E32 + ((long long)bi * a.S + i) * nn;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) E32[e] = (float)Ep[(e / n) * ld + e % n];
+  }
+  // row r: four threads per row, strided columns, combined by shuffles
+  double rmax = 0.0;
+  const int q = threadIdx.x & 3;
+  for (int r0 = threadIdx.x >> 2; r0 < ((n + 7) / 8) * 8; r0 += blockDim.x >> 2) {
+    const int r = r0 < n ? r0 : n - 1;
+    double sum = 0.0;
+    for (int c = q; c < n; c += 4)
+      sum += fabs(c <= r ? Ls[r * ld + c] : Ls[c * ld + r]) + fabs(Em[r * ld + c]) + fabs(Ep[c * ld + r]);
+    sum += __shfl_xor_sync(kFull, sum, 1);
+    sum += __shfl_xor_sync(kFull, sum, 2);
+    if (r0 < n) rmax = fmax(rmax, sum);
+  }
+  const double bm = block_max(bmax, red);
+  const double pm = block_max(rmax, red);
+  if (threadIdx.x == 0) {
+    atomic_max_pos(&a.st[bi].bnorm, bm);
+    atomic_max_pos(&a.st[bi].psi, pm);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ref_init_rows(RefineArgs a) {
+  const int per = a.N > a.S ? a.N : a.S;
+  const int bi = blockIdx.x / per;
+  const int i = blockIdx.x - bi * per;
+  if (a.mask != nullptr && a.mask[bi] == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ref_init_rows_body(a, bi, i, smem_raw);
+}
+
 // Convergence test per instance; clears the accumulators for the next round.
 // A non-finite eta (numerical breakdown of the float factor) stops the
 // instance with iters = -(iterations done).
