@@ -284,6 +284,7 @@ def run_ours(args, rank, world, local_rank):
     del e2e_run, Ld, Ed, bd, xd, Lw, Ew, xw, L32, E32, x32, b32
     torch.cuda.empty_cache()
     rg = bench_ragged(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
+    ad = bench_autograd(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
     barrier()
     sampler.__exit__(None, None, None)
     if rank != 0:
@@ -334,6 +335,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if rg is not None:
         line["ragged"] = rg
+    if ad is not None:
+        line["autograd"] = ad
     print(json.dumps(line), flush=True)
 
 
@@ -385,13 +388,42 @@ def bench_ragged(dev, steps, time_steps, agg):
     return out
 
 
+def bench_autograd(dev, steps, time_steps, agg):
+    """Differentiable solve on 256 systems of N=128, n=16, m=1 (FP64): forward
+    solve, loss = sum(w * x), backward (adjoint solve on the stored factor and
+    the fused dD/dE kernel).  A step is one forward + backward pass."""
+    import torch
+
+    from socu_b200.autograd import block_tridiag_solve
+    from socu_b200.problems import readme_blocks
+
+    B, N, n, m = 256, 128, 16, 1
+    L, E, b = readme_blocks(N, n, m, shift=10.0, seed=SEED, batch=B, device=dev)
+    D = L.clone().requires_grad_(True)
+    Ec = E[:, :N - 1].clone().requires_grad_(True)
+    bb = b.clone().requires_grad_(True)
+    w = torch.randn(B, N, n, m, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
+
+    def step():
+        D.grad = Ec.grad = bb.grad = None
+        x = block_tridiag_solve(D, Ec, bb)
+        (w * x).sum().backward()
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize(dev)
+    sec = agg(time_steps(step, lambda: None, max(3, steps // 2)))
+    return {"workload": "256 systems, N=128, n=16, m=1, FP64, loss = sum(w*x), forward + backward",
+            "value": B / sec, "unit": "solves/s (forward + backward)", "ms_per_step": sec * 1e3}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch measurement")
+    ap.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch and autograd measurements")
     ap.add_argument("--profile", action="store_true",
                     help="for profiler runs only: the mixed solve runs without its CUDA graph")
     args = ap.parse_args()

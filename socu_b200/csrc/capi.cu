@@ -360,8 +360,10 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
     const size_t srow = smem_residual_rows_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
-    if (e == cudaSuccess) e = prepare(k_residual_rows<true>, srow);
-    if (e == cudaSuccess) e = prepare(k_ref_init_rows, srow);
+    if (residual_uses_rows(a.n)) {
+      if (e == cudaSuccess) e = prepare(k_residual_rows<true>, srow);
+      if (e == cudaSuccess) e = prepare(k_ref_init_rows, srow);
+    }
     if (e != cudaSuccess) return cuda_status(e);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
     const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
@@ -879,8 +881,10 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
   const size_t srow = smem_residual_rows_elems(n) * sizeof(double);
-  if (e == cudaSuccess) e = noalloc_smem(k_residual_rows<true>, srow);
-  if (e == cudaSuccess) e = noalloc_smem(k_ref_init_rows, srow);
+  if (residual_uses_rows(n)) {
+    if (e == cudaSuccess) e = noalloc_smem(k_residual_rows<true>, srow);
+    if (e == cudaSuccess) e = noalloc_smem(k_ref_init_rows, srow);
+  }
   if (e != cudaSuccess) return cuda_status(e);
   (void)0;
   const int nrc = ceil_div(n, kResRows);
