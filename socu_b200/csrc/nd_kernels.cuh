@@ -482,32 +482,97 @@ __device__ void sweep_upper_solve(T* Y, int ldy, int mc, const T* __restrict__ L
 // a node sit in shared memory (one load round), Y/Z are n x mc column chunks.
 // Leading dimensions are even so every load can be vectorised.
 // ---------------------------------------------------------------------------
+// vector leading dimension of the resident sweeps: rows start on 16 bytes and
+// every 8-column pass can read 8 elements past its first column
+__host__ __device__ inline int res_ldy(int mc) { return ((mc + 3) / 4) * 4 + 4; }
 __host__ __device__ inline long long smem_sweep_res_elems(int n, int m) {
   const int mc = min_i(m, kMC);
-  return 3LL * n * even_ld(n) + 3LL * n * even_ld(mc) + n;
+  return 3LL * n * even_ld(n) + 3LL * n * res_ldy(mc) + n;
 }
 
-// Y -= op(M) Z, M resident (ld ldm).  TRANS: out[r][c] = sum_k M[k][r] Z[k][c].
-// One thread per output, four independent partial sums.
-template <typename T, bool TRANS>
-__device__ __forceinline__ void res_accumulate(T* Y, const T* Z, int ldy, int mc, const T* M, int ldm, int n) {
-  for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
-    const int r = o / mc, c = o - r * mc;
-    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
-    int k = 0;
-    for (; k + 3 < n; k += 4) {
-      const T m0 = TRANS ? M[k * ldm + r] : M[r * ldm + k];
-      const T m1 = TRANS ? M[(k + 1) * ldm + r] : M[r * ldm + k + 1];
-      const T m2 = TRANS ? M[(k + 2) * ldm + r] : M[r * ldm + k + 2];
-      const T m3 = TRANS ? M[(k + 3) * ldm + r] : M[r * ldm + k + 3];
-      s0 = fma(m0, Z[k * ldy + c], s0);
-      s1 = fma(m1, Z[(k + 1) * ldy + c], s1);
-      s2 = fma(m2, Z[(k + 2) * ldy + c], s2);
-      s3 = fma(m3, Z[(k + 3) * ldy + c], s3);
+// CW consecutive elements from 16-byte-aligned shared memory (8-byte for CW = 2 floats)
+template <typename T, int CW>
+__device__ __forceinline__ void load_cols(const T* p, T (&v)[CW]) {
+  if constexpr (CW == 1) {
+    v[0] = p[0];
+  } else if constexpr (sizeof(T) == 4 && CW == 2) {
+    const float2 a = *reinterpret_cast<const float2*>(p);
+    v[0] = a.x; v[1] = a.y;
+  } else if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int h = 0; h < CW / 4; ++h) {
+      const float4 a = *reinterpret_cast<const float4*>(p + 4 * h);
+      v[4 * h] = a.x; v[4 * h + 1] = a.y; v[4 * h + 2] = a.z; v[4 * h + 3] = a.w;
     }
-    for (; k < n; ++k) s0 = fma(TRANS ? M[k * ldm + r] : M[r * ldm + k], Z[k * ldy + c], s0);
-    Y[r * ldy + c] -= (s0 + s1) + (s2 + s3);
+  } else {
+#pragma unroll
+    for (int h = 0; h < CW / 2; ++h) {
+      const double2 a = *reinterpret_cast<const double2*>(p + 2 * h);
+      v[2 * h] = a.x; v[2 * h + 1] = a.y;
+    }
   }
+}
+
+// Resident block times resident vectors, n <= 64 rows, up to kMC columns:
+//   MODE 0: Yout -= M Z            M(r,k) = M[r*ldm + k]
+//   MODE 1: Yout -= M^T Z          M(r,k) = M[k*ldm + r]
+//   MODE 2: Yout = W^T Z           W^T(r,k) = M[r*ldm + k] for k > r, diagonal dv[r]
+//   MODE 3: Yout = W Z             W(r,k) = M[k*ldm + r] for k < r, diagonal dv[r]
+// (modes 2/3 read the inverse W = C^{-1} that an inverse-carrying factor keeps
+// in its strict upper triangle).  Four consecutive threads share a row and
+// split its contraction; each holds CW output columns in registers (CW = 8,
+// 4, 2 or 1 by the column count), reads Z rows with vector loads (rows are
+// 16-byte aligned, ldy from res_ldy) and the four partial rows are combined
+// with two shuffles.
+template <typename T, int MODE, int CW>
+__device__ __forceinline__ void res_rowdot(T* Yout, const T* Z, int ldy, int mc, const T* M, int ldm, const T* dv,
+                                           int n) {
+  const int q = threadIdx.x & 3;
+  const int nr = ((n + 7) / 8) * 8;   // whole warps iterate together (shuffles)
+  for (int c0 = 0; c0 < mc; c0 += CW) {
+    for (int rb = threadIdx.x >> 2; rb < nr; rb += blockDim.x >> 2) {
+      const int r = rb < n ? rb : n - 1;
+      T acc[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) acc[j] = T(0);
+      const int k0 = MODE == 2 ? r + 1 : 0, k1 = MODE == 3 ? r : n;
+      for (int k = k0 + q; k < k1; k += 4) {
+        const T mv = (MODE == 0 || MODE == 2) ? M[r * ldm + k] : M[k * ldm + r];
+        T z[CW];
+        load_cols<T, CW>(Z + k * ldy + c0, z);
+#pragma unroll
+        for (int j = 0; j < CW; ++j) acc[j] = fma(mv, z[j], acc[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        acc[j] += __shfl_xor_sync(kFull, acc[j], 1);
+        acc[j] += __shfl_xor_sync(kFull, acc[j], 2);
+      }
+      if (rb < n) {
+#pragma unroll
+        for (int j = 0; j < CW; ++j) {
+          if ((j & 3) != q || c0 + j >= mc) continue;
+          if (MODE <= 1)
+            Yout[r * ldy + c0 + j] -= acc[j];
+          else
+            Yout[r * ldy + c0 + j] = dv[r] * Z[r * ldy + c0 + j] + acc[j];
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ void res_matvec(T* Yout, const T* Z, int ldy, int mc, const T* M, int ldm, const T* dv,
+                                           int n) {
+  if (mc >= 8)
+    res_rowdot<T, MODE, 8>(Yout, Z, ldy, mc, M, ldm, dv, n);
+  else if (mc >= 4)
+    res_rowdot<T, MODE, 4>(Yout, Z, ldy, mc, M, ldm, dv, n);
+  else if (mc >= 2)
+    res_rowdot<T, MODE, 2>(Yout, Z, ldy, mc, M, ldm, dv, n);
+  else
+    res_rowdot<T, MODE, 1>(Yout, Z, ldy, mc, M, ldm, dv, n);
 }
 
 // Y <- C^{-1} Y (UPPER: Y <- C^{-T} Y), C = lower(Cs) resident, dv[r] = 1/C[r][r].
@@ -574,27 +639,6 @@ __device__ void res_tri_solve(T* Y, int ldy, int mc, const T* Cs, int ldc, const
 // Every vector has one writer per launch (K launches per forward sweep).
 // RES: factor and coupling blocks resident in shared memory.
 // ---------------------------------------------------------------------------
-// Y_out = W Y (UPPER: W^T Y) with W = C^{-1} kept as in k_node<INV>:
-// W[r][k] = Ls[k][r] (k < r), W[r][r] = dv[r].  Parallel matvec.
-template <typename T, bool UPPER>
-__device__ __forceinline__ void res_inv_apply(T* Yout, const T* Y, int ldy, int mc, const T* Ls, int ldm,
-                                              const T* dv, int n) {
-  for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
-    const int r = o / mc, c = o - r * mc;
-    T s0 = dv[r] * Y[r * ldy + c], s1 = T(0), s2 = T(0), s3 = T(0);
-    const int k0 = UPPER ? r + 1 : 0, k1 = UPPER ? n : r;
-    int k = k0;
-    for (; k + 3 < k1; k += 4) {
-      s0 = fma(UPPER ? Ls[r * ldm + k] : Ls[k * ldm + r], Y[k * ldy + c], s0);
-      s1 = fma(UPPER ? Ls[r * ldm + k + 1] : Ls[(k + 1) * ldm + r], Y[(k + 1) * ldy + c], s1);
-      s2 = fma(UPPER ? Ls[r * ldm + k + 2] : Ls[(k + 2) * ldm + r], Y[(k + 2) * ldy + c], s2);
-      s3 = fma(UPPER ? Ls[r * ldm + k + 3] : Ls[(k + 3) * ldm + r], Y[(k + 3) * ldy + c], s3);
-    }
-    for (; k < k1; ++k) s0 = fma(UPPER ? Ls[r * ldm + k] : Ls[k * ldm + r], Y[k * ldy + c], s0);
-    Yout[r * ldy + c] = (s0 + s1) + (s2 + s3);
-  }
-}
-
 // PULL_ONLY (fused factor_and_solve): apply the updates, never solve.
 // INV (resident only): the factor carries its inverse (k_node<INV>), the
 // triangular solve becomes a matvec.
@@ -621,7 +665,7 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
     F = p.Eb(b, lv.op + 2 * u - 2);
     if (j + h < N) G = p.Eb(b, lv.op + 2 * u - 1);
   }
-  const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
@@ -650,14 +694,14 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
       if (c0 == 0 && solve)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
       if (pull) {
-        res_accumulate<T, false>(Y, Z1, ldy, mc, Fs, ldm, n);          // Y -= F y_{j-h}
+        res_matvec<T, 0>(Y, Z1, ldy, mc, Fs, ldm, nullptr, n);          // Y -= F y_{j-h}
         __syncthreads();
-        if (G) res_accumulate<T, true>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G^T y_{j+h}
+        if (G) res_matvec<T, 1>(Y, Z2, ldy, mc, Gs, ldm, nullptr, n);   // Y -= G^T y_{j+h}
       }
       __syncthreads();
       if (solve) {
         if (INV) {
-          res_inv_apply<T, false>(Z2, Y, ldy, mc, Cs, ldm, dv, n);
+          res_matvec<T, 3>(Z2, Y, ldy, mc, Cs, ldm, dv, n);
           __syncthreads();
           store_block(yj + c0, p.m, Z2, ldy, n, mc);
           continue;
@@ -693,7 +737,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
                                          unsigned char* smem_raw) {
   const int n = p.n, s = lv.s, N = p.N;
   const int i = s - 1 + 2 * s * t;
-  const int mcmax = min_i(p.m, kMC), ldy = RES ? even_ld(mcmax) : mcmax + 1;
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : mcmax + 1;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
@@ -724,12 +768,12 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
     if (RES) {
       if (c0 == 0)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
-      if (right) res_accumulate<T, true>(Y, Z1, ldy, mc, Fs, ldm, n);    // Y -= F^T x_{i+s}
+      if (right) res_matvec<T, 1>(Y, Z1, ldy, mc, Fs, ldm, nullptr, n);   // Y -= F^T x_{i+s}
       __syncthreads();
-      if (left) res_accumulate<T, false>(Y, Z2, ldy, mc, Gs, ldm, n);    // Y -= G x_{i-s}
+      if (left) res_matvec<T, 0>(Y, Z2, ldy, mc, Gs, ldm, nullptr, n);    // Y -= G x_{i-s}
       __syncthreads();
       if (INV) {
-        res_inv_apply<T, true>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
+        res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
         __syncthreads();
         store_block(xi + c0, p.m, Z1, ldy, n, mc);
         continue;
