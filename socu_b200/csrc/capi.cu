@@ -128,11 +128,35 @@ bool use_inverse(int n, int m) {
                         (long long)max_smem_optin();
 }
 
+// Second stream and two events for graph capture: inside factor_and_solve,
+// each level's forward pull runs on a parallel branch beside the Schur update
+// (both only depend on the level's node kernel).
+struct Fork {
+  cudaStream_t aux = nullptr;
+  cudaEvent_t split = nullptr, join = nullptr;
+  bool ok() const { return aux && split && join; }
+  int create() {
+    cudaError_t e = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&split, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    return cuda_status(e);
+  }
+  void destroy() {
+    if (aux) cudaStreamDestroy(aux);
+    if (split) cudaEventDestroy(split);
+    if (join) cudaEventDestroy(join);
+    aux = nullptr;
+    split = join = nullptr;
+  }
+};
+
 // Enqueue (or count, when st == nullptr and count != nullptr) the kernels of one op.
 // inv: the factor carries (FACTOR, FACTOR_AND_SOLVE) or has (SOLVE) its
 // diagonal inverses; only for internal factors or within factor_and_solve.
+// fork (graph capture only): run the forward pulls on a parallel branch.
 template <typename T>
-int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, bool inv = false) {
+int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, bool inv = false,
+            const Fork* fork = nullptr) {
   const std::vector<Level> lv = schedule(p.N);
   const int K = static_cast<int>(lv.size());
   const int n = p.n, nth = threads_for(n);
@@ -164,11 +188,15 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     if (e != cudaSuccess) return cuda_status(e);
   }
 
-  auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
+  auto go_on = [&](cudaStream_t s, auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
     if (blocks <= 0) return;
     ++launches;
-    if (run) kernel<<<(unsigned)blocks, threads > 0 ? threads : nth, smem, st>>>(p, L);
+    if (run) kernel<<<(unsigned)blocks, threads > 0 ? threads : nth, smem, s>>>(p, L);
   };
+  auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
+    go_on(st, kernel, blocks, smem, L, threads);
+  };
+  const bool forked = run && fork != nullptr && fork->ok();
 
   const bool factor = op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (factor) {
@@ -176,10 +204,19 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       const Level& L = lv[l];
       go(node_kernel, (long long)p.B * L.d, sd, L, nth);
       if (l + 1 < K) {
-        const int U = p.N / (2 * L.s);
-        go(k_update<T>, (long long)p.B * update_launch_tasks(n, p.N, L), su, L);
         // fused forward: apply this level's updates to every target vector
-        if (withY) go(pull_kernel, (long long)p.B * (p.N / lv[l + 1].s), ss, lv[l + 1]);
+        const long long pull_blocks = withY ? (long long)p.B * (p.N / lv[l + 1].s) : 0;
+        if (forked && pull_blocks > 0) {
+          cudaEventRecord(fork->split, st);
+          cudaStreamWaitEvent(fork->aux, fork->split, 0);
+          go_on(fork->aux, pull_kernel, pull_blocks, ss, lv[l + 1]);
+          cudaEventRecord(fork->join, fork->aux);
+        }
+        go(k_update<T>, (long long)p.B * update_launch_tasks(n, p.N, L), su, L);
+        if (forked && pull_blocks > 0)
+          cudaStreamWaitEvent(st, fork->join, 0);
+        else
+          go(pull_kernel, pull_blocks, ss, lv[l + 1]);
       }
     }
   }
@@ -247,7 +284,7 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
 
 int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask,
              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, cudaStream_t st,
-             long long* count) {
+             long long* count, const Fork* fork = nullptr) {
   Dims d;
   const int v = validate(op, dtype, L, E, x, batch, horizon, n, n_rhs, &d);
   if (v != SOCU_OK) return v;
@@ -266,8 +303,8 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
   op = base_op(op, &inv);
   inv = inv || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (dtype == SOCU_FLOAT64)
-    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv);
-  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv);
+    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv, fork);
+  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv, fork);
 }
 
 
@@ -351,7 +388,7 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
 // Mixed solve, part 1: state reset, float copies, norms, then the first
 // round fused into the float factor: factor_and_solve on R32 = b gives
 // delta = x_1, followed by x += delta, the FP64 residual and the test.
-int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
+int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, const Fork* fork = nullptr) {
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
@@ -375,7 +412,7 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count) {
     if (e != cudaSuccess) return cuda_status(e);
   }
   long long c = 0, cr = 0;
-  int s = enqueue<float>(SOCU_OP_FACTOR_AND_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
+  int s = enqueue<float>(SOCU_OP_FACTOR_AND_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m), fork);
   if (s != SOCU_OK) return s;
   s = refine_finish_round(a, st, run ? nullptr : &cr);
   if (count) *count = 2 + c + cr;
@@ -427,7 +464,9 @@ int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
     st = cuda_status(e);
     capturing = st == SOCU_OK;
   }
-  if (st == SOCU_OK) st = refine_prologue(a, cap, nullptr);
+  Fork fork;
+  if (st == SOCU_OK) st = fork.create();
+  if (st == SOCU_OK) st = refine_prologue(a, cap, nullptr, &fork);
   cudaGraph_t g = nullptr;
   cudaGraphConditionalHandle hnd = 0;
   cudaGraphNode_t node = nullptr;
@@ -476,6 +515,7 @@ int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
   }
   if (cap) cudaStreamDestroy(cap);
   if (body) cudaStreamDestroy(body);
+  fork.destroy();
   if (st != SOCU_OK) {
     if (fin) cudaGraphDestroy(fin);
     return st;
@@ -747,8 +787,8 @@ int rg_refine_solve(socu_ragged_s* r, const double* L, const double* E, const do
   return rg_launch<float, kRgRefine>(r, a, st);
 }
 
-// enqueue one run of a launch object on `st`
-int launch_enqueue(socu_launch_s* h, cudaStream_t st) {
+// enqueue one run of a launch object on `st` (fork: graph capture only)
+int launch_enqueue(socu_launch_s* h, cudaStream_t st, const Fork* fork = nullptr) {
   if (h->rg) {
     if (h->rg->refine)
       return rg_refine_solve(h->rg, static_cast<const double*>(h->L), static_cast<const double*>(h->E), h->b,
@@ -761,7 +801,8 @@ int launch_enqueue(socu_launch_s* h, cudaStream_t st) {
     if (e != cudaSuccess) return cuda_status(e);
     return refine_enqueue(h->ra, st, nullptr);
   }
-  return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st, nullptr);
+  return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st, nullptr,
+                  fork);
 }
 
 // Capture one run into a CUDA graph on a private stream (the legacy default
@@ -777,9 +818,11 @@ int capture(socu_launch_s* h) {
   cudaStream_t cap = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
   int st = SOCU_OK;
+  Fork fork;
+  if (e == cudaSuccess && fork.create() != SOCU_OK) e = static_cast<cudaError_t>(g_last_cuda_error);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    st = launch_enqueue(h, cap);
+    st = launch_enqueue(h, cap, &fork);
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(cap, &g);
     if (st == SOCU_OK && e2 != cudaSuccess) st = cuda_status(e2);
@@ -789,6 +832,7 @@ int capture(socu_launch_s* h) {
     st = cuda_status(e);
   }
   if (cap) cudaStreamDestroy(cap);
+  fork.destroy();
   if (st != SOCU_OK) {
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);

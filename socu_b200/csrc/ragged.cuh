@@ -139,7 +139,7 @@ __host__ __device__ inline RgPhase rg_phase(const RgInst& I, int mode, int ph) {
     r.kind = kRgXupd;
     r.level = 0;
     r.units = I.N;
-    r.upc = I.N;   // one chunk: the update is a short elementwise pass
+    r.upc = 16;    // 16 blocks per chunk: a short elementwise pass
   } else {
     r.kind = kRgRes;
     r.level = 0;
@@ -293,9 +293,10 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
   constexpr bool kPlain = MODE == kRgPlain;
   if (P.kind == kRgXupd) {
     if constexpr (!kPlain) {
-      const float* d = reinterpret_cast<const float*>(a.X) + I.oX;
-      double* x = a.x64 + I.oX;
-      const long long len = (long long)I.N * I.n * I.m;
+      const long long per = (long long)I.n * I.m;
+      const float* d = reinterpret_cast<const float*>(a.X) + I.oX + u0 * per;
+      double* x = a.x64 + I.oX + u0 * per;
+      const long long len = (long long)(u1 - u0) * per;
       for (long long e = threadIdx.x; e < len; e += blockDim.x) x[e] += (double)d[e];
     }
     return;
