@@ -576,7 +576,7 @@ namespace {
 // ragged batches
 // ---------------------------------------------------------------------------
 constexpr int kRgMaxBlock = 64;                 // resident sweeps with diagonal inverses
-constexpr int kRgThreads = 256;
+constexpr int kRgThreads = 128;   // 3 CTAs per SM at n = 48 (shared-memory bound) instead of 2
 constexpr long long kRgTimeoutNs = 4000000000LL;   // bound of one queue wait (4 s)
 
 int rg_upc(int n) { return n <= 8 ? 8 : (n <= 16 ? 4 : (n <= 32 ? 2 : 1)); }
