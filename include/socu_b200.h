@@ -156,6 +156,24 @@ int socu_refine_launch_create(socu_launch_t* out, const double* L, const double*
                               int max_iter, double tol, void* workspace, size_t workspace_bytes, double* eta,
                               int32_t* iters, int use_cuda_graph, void* stream);
 
+/* Graph-captured refined solve with an FP64 fallback (no counterpart in the
+ * reference).  After the refinement loop, every active instance whose eta did
+ * not reach tol -- refinement stalled, ran out of max_iter rounds, or the
+ * float factor broke down -- is solved again by the plain FP64
+ * factor_and_solve on working copies of its original blocks, and its eta is
+ * recomputed; this stage sits in a conditional IF graph node that runs only
+ * when some instance needs it.  used_fp64 (batch,) device output: 1 where x
+ * comes from the FP64 path.  iters keeps the refinement count (negative on
+ * breakdown).  The workspace (>= socu_refine_fallback_workspace_bytes,
+ * 256-byte aligned) adds FP64 copies of L and E to the refinement workspace. */
+size_t socu_refine_fallback_workspace_bytes(int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs);
+
+int socu_refine_fallback_launch_create(socu_launch_t* out, const double* L, const double* E, const double* b,
+                                       double* x, const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n,
+                                       int64_t n_rhs, int max_iter, double tol, void* workspace,
+                                       size_t workspace_bytes, double* eta, int32_t* iters, uint8_t* used_fp64,
+                                       void* stream);
+
 /* Same solve as socu_refine_solve, for callers that cannot allocate device
  * memory while they solve: an XLA/JAX custom call (buffers come from XLA's
  * allocator, the handler must not cudaMalloc), a real-time control loop that

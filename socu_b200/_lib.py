@@ -68,6 +68,10 @@ _SIGNATURES = {
                                  _vp, ctypes.c_size_t, _vp, _vp, _vp]),
     "socu_refine_launch_create": (_int, [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64,
                                          _int, ctypes.c_double, _vp, ctypes.c_size_t, _vp, _vp, _int, _vp]),
+    "socu_refine_fallback_workspace_bytes": (ctypes.c_size_t, [_i64, _i64, _i64, _i64]),
+    "socu_refine_fallback_launch_create": (_int, [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64,
+                                                  _i64, _int, ctypes.c_double, _vp, ctypes.c_size_t, _vp, _vp, _vp,
+                                                  _vp]),
     "socu_block_tridiag_residual": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "socu_block_tridiag_grad": (_int, [_int, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
     "socu_refine_solve_noalloc": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,

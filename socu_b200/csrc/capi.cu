@@ -331,6 +331,23 @@ RefineLayout refine_layout(int64_t B, int64_t N, int64_t n, int64_t m) {
   return o;
 }
 
+// Fallback workspace: the refinement workspace, then the FP64 working copies.
+struct FallbackLayout {
+  size_t l64, e64, fb, any, total;
+};
+
+FallbackLayout fallback_layout(int64_t B, int64_t N, int64_t n, int64_t m) {
+  FallbackLayout o;
+  const int64_t S = socu_off_diag_storage_len(N);
+  size_t off = refine_layout(B, N, n, m).total;
+  o.l64 = off; off += align256((size_t)B * N * n * n * sizeof(double));
+  o.e64 = off; off += align256((size_t)B * (S > 0 ? S : 0) * n * n * sizeof(double));
+  o.fb = off; off += align256((size_t)B);
+  o.any = off; off += align256(sizeof(int));
+  o.total = off;
+  return o;
+}
+
 int refine_validate(const void* L, const void* E, const void* b, void* x, int64_t batch, int64_t horizon,
                     int64_t n, int64_t n_rhs, int max_iter, double tol, void* ws, size_t ws_bytes,
                     const double* eta, const int32_t* iters, Dims* d) {
@@ -453,7 +470,58 @@ int refine_enqueue(const RefineArgs& a, cudaStream_t st, long long* count) {
 // Capture the mixed solve into a graph whose refinement rounds sit in a
 // conditional WHILE node: the loop stops as soon as every instance has
 // converged (or hit max_iter), instead of launching max_iter rounds.
-int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
+// FP64 fallback stage, appended after the loop: select, IF node (copy, FP64
+// factor_and_solve, residual, eta).
+int capture_fallback(const RefineArgs& a, const FallbackArgs& f, cudaStream_t cap, cudaStream_t body) {
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle hnd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(cap, &cs, nullptr, &g, &deps, &nd);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, g, 0, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f.any, 0, sizeof(int), cap);
+  if (e != cudaSuccess) return cuda_status(e);
+  const int chk_blocks = (a.B + 255) / 256;
+  k_fb_select<<<chk_blocks, 256, 0, cap>>>(a, f);
+  k_fb_decide<<<1, 1, 0, cap>>>(hnd, f.any);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cap, &cs, nullptr, &g, &deps, &nd);
+  cudaGraphNodeParams prm = {};
+  prm.type = cudaGraphNodeTypeConditional;
+  prm.conditional.handle = hnd;
+  prm.conditional.type = cudaGraphCondTypeIf;
+  prm.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &prm);
+  if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(body, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_status(e);
+  const unsigned copy_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
+  k_fb_copy<<<copy_blocks, 256, 0, body>>>(a, f);
+  const Dims d{a.B, a.N, a.n, a.m, a.S};
+  int st = enqueue<double>(SOCU_OP_FACTOR_AND_SOLVE, make_problem<double>(f.L64, f.E64, a.x, f.fb, d), body, nullptr,
+                           true);
+  RefineArgs ra = a;
+  ra.active = f.fb;
+  if (st == SOCU_OK) {
+    if (residual_uses_rows(a.n))
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, smem_residual_rows_elems(a.n) * sizeof(double),
+                              body>>>(ra);
+    else
+      k_residual<true><<<(unsigned)((long long)a.B * a.N * ceil_div(a.n, kResRows)), 256,
+                         smem_residual_elems(a.n) * sizeof(double), body>>>(ra);
+    k_fb_eta<<<chk_blocks, 256, 0, body>>>(a, f);
+  }
+  cudaGraph_t bg = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(body, &bg);
+  if (st == SOCU_OK) st = cuda_status(e2 != cudaSuccess ? e2 : cudaGetLastError());
+  return st;
+}
+
+int capture_refine_while(const RefineArgs& a, cudaGraph_t* out, const FallbackArgs* fallback = nullptr) {
   cudaStream_t cap = nullptr, body = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking);
@@ -508,6 +576,7 @@ int capture_refine_while(const RefineArgs& a, cudaGraph_t* out) {
       if (st == SOCU_OK) st = cuda_status(e2 != cudaSuccess ? e2 : cudaGetLastError());
     }
   }
+  if (st == SOCU_OK && fallback != nullptr) st = capture_fallback(a, *fallback, cap, body);
   cudaGraph_t fin = nullptr;
   if (capturing) {
     const cudaError_t e3 = cudaStreamEndCapture(cap, &fin);
@@ -1228,6 +1297,76 @@ int socu_refine_launch_create(socu_launch_t* out, const double* L, const double*
     h->kernels = cp + 1;
     h->round_kernels = ci + 1;
   }
+  (void)stream;
+  *out = h;
+  return SOCU_OK;
+}
+
+size_t socu_refine_fallback_workspace_bytes(int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs) {
+  if (batch < 0 || horizon <= 0 || n <= 0 || n_rhs <= 0) return 0;
+  return fallback_layout(batch, horizon, n, n_rhs).total;
+}
+
+int socu_refine_fallback_launch_create(socu_launch_t* out, const double* L, const double* E, const double* b,
+                                       double* x, const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n,
+                                       int64_t n_rhs, int max_iter, double tol, void* workspace,
+                                       size_t workspace_bytes, double* eta, int32_t* iters, uint8_t* used_fp64,
+                                       void* stream) {
+  if (out == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  Dims d;
+  int st = refine_validate(L, E, b, x, batch, horizon, n, n_rhs, max_iter, tol, workspace, workspace_bytes, eta,
+                           iters, &d);
+  if (st != SOCU_OK) return st;
+  if (batch > 0) {
+    if (used_fp64 == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+    if (workspace_bytes < fallback_layout(batch, horizon, n, n_rhs).total) return SOCU_ERR_INVALID_ARGUMENT;
+    Dims d64;
+    const int v = validate(SOCU_OP_FACTOR_AND_SOLVE, SOCU_FLOAT64, L, E, x, batch, horizon, n, n_rhs, &d64);
+    if (v != SOCU_OK) return v;
+  }
+  socu_launch_s* h = new (std::nothrow) socu_launch_s();
+  if (!h) return SOCU_ERR_UNSUPPORTED;
+  h->op = SOCU_OP_SOLVE;
+  h->dtype = SOCU_FLOAT64;
+  h->L = const_cast<double*>(L);
+  h->E = const_cast<double*>(E);
+  h->x = x;
+  h->mask = mask;
+  h->batch = batch;
+  h->horizon = horizon;
+  h->n = n;
+  h->n_rhs = n_rhs;
+  h->graph = nullptr;
+  h->exec = nullptr;
+  h->refine = true;
+  if (batch == 0) {
+    *out = h;
+    return SOCU_OK;
+  }
+  h->ra = refine_args(L, E, b, x, mask, d, max_iter, tol, workspace, eta, iters);
+  const FallbackLayout lay = fallback_layout(batch, horizon, n, n_rhs);
+  char* w = static_cast<char*>(workspace);
+  FallbackArgs f;
+  f.L64 = reinterpret_cast<double*>(w + lay.l64);
+  f.E64 = reinterpret_cast<double*>(w + lay.e64);
+  f.fb = reinterpret_cast<uint8_t*>(w + lay.fb);
+  f.any = reinterpret_cast<int*>(w + lay.any);
+  f.used = used_fp64;
+  st = cuda_status(ensure_device(L));
+  if (st == SOCU_OK) st = capture_refine_while(h->ra, &h->graph, &f);
+  if (st == SOCU_OK) st = cuda_status(cudaGraphInstantiate(&h->exec, h->graph, 0));
+  if (st != SOCU_OK) {
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    delete h;
+    return st;
+  }
+  long long cp = 0, ci = 0;
+  refine_prologue(h->ra, nullptr, &cp);
+  refine_iteration(h->ra, nullptr, &ci);
+  h->kernels = cp + 1 + 2;   // prologue, loop test, fallback select + decide
+  h->round_kernels = ci + 1;
   (void)stream;
   *out = h;
   return SOCU_OK;

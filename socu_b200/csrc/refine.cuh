@@ -437,6 +437,79 @@ __global__ void k_ref_check(RefineArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 fallback after refinement (graph-captured solve only).  Instances whose
+// refinement did not reach tol -- it stalled, ran out of rounds, or the float
+// factor broke down -- are solved again by the plain FP64 factor_and_solve on
+// working copies of their original blocks, inside a conditional IF node that
+// runs only when some instance needs it.
+// ---------------------------------------------------------------------------
+struct FallbackArgs {
+  double* L64;     // (B, N, n, n) FP64 working copy of L
+  double* E64;     // (B, S, n, n) FP64 working copy of E (slots >= N-1 zero)
+  uint8_t* fb;     // per instance: solved again in FP64 (the FP64 solve's batch mask)
+  int* any;        // 1 when some instance is in fb
+  uint8_t* used;   // caller output (B,): 1 where x comes from the FP64 path
+};
+
+__global__ void k_fb_select(RefineArgs a, FallbackArgs f) {
+  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
+    const bool on = a.mask == nullptr || a.mask[bi] != 0;
+    const bool fail = on && !(a.eta[bi] <= a.tol);
+    f.fb[bi] = fail ? 1 : 0;
+    f.used[bi] = fail ? 1 : 0;
+    if (fail) atomicExch(f.any, 1);
+  }
+}
+
+// IF-node condition: run the FP64 stage when some instance needs it.
+__global__ void k_fb_decide(cudaGraphConditionalHandle h, int* any) {
+  const int v = *any;
+  *any = 0;
+  cudaGraphSetConditional(h, v ? 1u : 0u);
+}
+
+// One CTA per (instance, block index i < max(N, S)) of the selected
+// instances: FP64 copies of L_i and slot i (zero for slots >= N-1), x_i = b_i.
+__global__ void __launch_bounds__(256) k_fb_copy(RefineArgs a, FallbackArgs f) {
+  const int per = a.N > a.S ? a.N : a.S;
+  const int bi = blockIdx.x / per;
+  const int i = blockIdx.x - bi * per;
+  if (!f.fb[bi]) return;
+  const long long nn = (long long)a.n * a.n;
+  if (i < a.N) {
+    const long long o = ((long long)bi * a.N + i) * nn;
+    for (long long e = threadIdx.x; e < nn; e += blockDim.x) f.L64[o + e] = a.L[o + e];
+    const long long v = ((long long)bi * a.N + i) * a.n * a.m;
+    for (long long e = threadIdx.x; e < (long long)a.n * a.m; e += blockDim.x) a.x[v + e] = a.b[v + e];
+  }
+  if (i < a.S) {
+    const long long o = ((long long)bi * a.S + i) * nn;
+    if (i < a.N - 1) {
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) f.E64[o + e] = a.E[o + e];
+    } else {
+      for (long long e = threadIdx.x; e < nn; e += blockDim.x) f.E64[o + e] = 0.0;
+    }
+  }
+}
+
+// Backward error of the FP64 solution (norms accumulated by the residual
+// kernel with fb as its instance mask).
+__global__ void k_fb_eta(RefineArgs a, FallbackArgs f) {
+  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
+    if (!f.fb[bi]) continue;
+    RefineState& s = a.st[bi];
+    const double rn = __longlong_as_double((long long)s.rnorm);
+    const double xn = __longlong_as_double((long long)s.xnorm);
+    const double pn = __longlong_as_double((long long)s.psi);
+    const double bn = __longlong_as_double((long long)s.bnorm);
+    const double den = pn * xn + bn;
+    a.eta[bi] = den > 0.0 ? rn / den : 0.0;
+    s.rnorm = 0ull;
+    s.xnorm = 0ull;
+  }
+}
+
 // Loop control for a graph WHILE node: keep iterating while some instance
 // is still active, and clear the flag for the next round.
 __global__ void k_ref_decide(cudaGraphConditionalHandle h, int* any_active) {

@@ -35,11 +35,19 @@ def _check_f64(**arrays):
 
 
 def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_iter=10, stream=None,
-                                         use_cuda_graph=True):
+                                         use_cuda_graph=True, fp64_fallback=False):
     """Returns a zero-argument callable solving Psi x = b (float factor + FP64
     refinement).  After each call, ``callback.eta`` (B,) holds the final
     backward errors and ``callback.iterations`` (B,) the corrections applied
-    (negative: the float factor broke down after that many steps)."""
+    (negative: the float factor broke down after that many steps).
+
+    fp64_fallback (graph only): instances whose refinement does not reach tol
+    (stalled, out of rounds, or broken down) are solved again by the plain
+    FP64 factor_and_solve inside the same graph; ``callback.used_fp64`` (B,)
+    marks them and ``callback.eta`` then holds the FP64 solution's backward
+    error.  Needs a workspace with FP64 copies of L and E."""
+    if fp64_fallback and not use_cuda_graph:
+        raise ValueError("fp64_fallback runs inside the CUDA graph; use_cuda_graph must be True")
     L, E, b, x = (_as_tensor(a) for a in (L, E, b, x))
     mask = _as_tensor(mask) if mask is not None else None
     assert b.shape == x.shape, "b and x must have the same shape"
@@ -48,20 +56,30 @@ def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_i
     _check_f64(L=L4, E=E4, b=b4, x=x4)
     dev = L4.device
     lib = _lib.load()
-    ws_bytes = int(lib.socu_refine_workspace_bytes(B, N, n, m))
+    ws_bytes = int(lib.socu_refine_fallback_workspace_bytes(B, N, n, m) if fp64_fallback
+                   else lib.socu_refine_workspace_bytes(B, N, n, m))
     ws = torch.empty(max(ws_bytes, 256) + 256, dtype=torch.uint8, device=dev)
     ws_ptr = (ws.data_ptr() + 255) // 256 * 256
     eta = torch.zeros(B, dtype=torch.float64, device=dev)
     iters = torch.zeros(B, dtype=torch.int32, device=dev)
     sh = _stream_handle(stream, dev)
     handle = ctypes.c_void_p()
+    used = torch.zeros(B, dtype=torch.uint8, device=dev)
     with torch.cuda.device(dev):
-        status = lib.socu_refine_launch_create(
-            ctypes.byref(handle), L4.data_ptr(), E4.data_ptr() if E4.numel() else None, b4.data_ptr(),
-            x4.data_ptr(), mask.data_ptr() if mask is not None else None, B, N, n, m, int(max_iter),
-            float(tol), ws_ptr, ws_bytes, eta.data_ptr(), iters.data_ptr(), int(bool(use_cuda_graph)),
-            sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream)
-    _lib.check(status, "socu_refine_launch_create")
+        cap_stream = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
+        E_ptr = E4.data_ptr() if E4.numel() else None
+        mask_ptr = mask.data_ptr() if mask is not None else None
+        if fp64_fallback:
+            status = lib.socu_refine_fallback_launch_create(
+                ctypes.byref(handle), L4.data_ptr(), E_ptr, b4.data_ptr(), x4.data_ptr(), mask_ptr, B, N, n, m,
+                int(max_iter), float(tol), ws_ptr, ws_bytes, eta.data_ptr(), iters.data_ptr(), used.data_ptr(),
+                cap_stream)
+        else:
+            status = lib.socu_refine_launch_create(
+                ctypes.byref(handle), L4.data_ptr(), E_ptr, b4.data_ptr(), x4.data_ptr(), mask_ptr, B, N, n, m,
+                int(max_iter), float(tol), ws_ptr, ws_bytes, eta.data_ptr(), iters.data_ptr(),
+                int(bool(use_cuda_graph)), cap_stream)
+    _lib.check(status, "socu_refine_fallback_launch_create" if fp64_fallback else "socu_refine_launch_create")
     h = handle.value
 
     def callback():
@@ -71,6 +89,7 @@ def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_i
     callback._socu_arrays = (L4, E4, b4, x4, mask, ws)
     callback.eta = eta
     callback.iterations = iters
+    callback.used_fp64 = used
     callback.workspace_bytes = ws_bytes
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     # graph mode: the refinement rounds run in a conditional WHILE node
