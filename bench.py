@@ -75,6 +75,17 @@ def algorithmic_factor_flops(N, n):
     return total
 
 
+def max_over_ranks(seconds, world, device):
+    """Step time of the whole job: the slowest rank's figure (every rank calls
+    this at the same points, in the same order)."""
+    import torch
+    import torch.distributed as dist
+    v = torch.tensor([seconds], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return float(v)
+
+
 # ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
@@ -325,10 +336,7 @@ def run_ours(args, rank, world, local_rank):
     del runs, bufs, xhs
 
     def agg(ts):
-        v = torch.tensor([statistics.mean(ts)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        return float(v)
+        return max_over_ranks(statistics.mean(ts), world, dev)
 
     sec_mixed, sec_plain, sec_fac, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_fac), agg(t_e2e)
     sec_e2e_serial = agg(t_e2e_serial)

@@ -27,7 +27,7 @@ import torch
 from . import _lib
 from .block_tridiag_solver import _stream_handle
 
-__all__ = ["RaggedBatch", "ragged_layout", "create_ragged_factor_and_solve_launch",
+__all__ = ["RaggedBatch", "ragged_layout", "shard_instances", "create_ragged_factor_and_solve_launch",
            "create_ragged_refined_solve_launch"]
 
 MAX_BLOCK_SIZE = 64
@@ -53,6 +53,21 @@ def ragged_layout(horizons, block_sizes, n_rhs):
     _lib.check(lib.socu_ragged_layout(_ptr(N), _ptr(n), _ptr(m), count, _ptr(off[0]), _ptr(off[1]),
                                       _ptr(off[2]), _ptr(tot)), "socu_ragged_layout")
     return off[0], off[1], off[2], tot
+
+
+def shard_instances(horizons, block_sizes, world_size, rank):
+    """Contiguous instance range [lo, hi) for `rank` when a ragged batch is
+    split over `world_size` GPUs (one process each), balanced by the factor
+    work N * n^3 of every instance.  Instances are independent, so the shards
+    need no exchange; each rank builds a RaggedBatch from its own range."""
+    assert world_size >= 1 and 0 <= rank < world_size, "rank must lie in [0, world_size)"
+    w = _i64(horizons).astype(np.float64) * _i64(block_sizes).astype(np.float64) ** 3
+    cum = np.concatenate([[0.0], np.cumsum(w)])
+    targets = cum[-1] * np.arange(world_size + 1) / world_size
+    bounds = np.searchsorted(cum, targets, side="left")
+    bounds[0], bounds[-1] = 0, len(w)
+    bounds = np.maximum.accumulate(bounds)
+    return int(bounds[rank]), int(bounds[rank + 1])
 
 
 class RaggedBatch:
