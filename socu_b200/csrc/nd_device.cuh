@@ -279,6 +279,132 @@ __device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restric
 
 
 // ---------------------------------------------------------------------------
+// Trailing update of one 8-column step of cta_chol_solve, both parts in one
+// tile loop (rows R0..n-1, P = A[R0.., K..K+kb) the solved panel):
+//   A22[r][c] -= sum_k P[r][k] P[c][k]        (c <= r; only when factoring)
+//   V[r][c]   -= sum_k P[r][k] V[K+k][c]      (c < nv)
+// The accumulators start from the target values and the panel operand is
+// negated, so a tile ends in a plain store.  FP64: DMMA warp tiles of 16 x 32
+// (fragment layout of mma.m8n8k4 .f64: a0 = A[g][t], b0 = B[t][g],
+// {c0, c1} = C[g][2t + {0, 1}], g = lane/4, t = lane%4).  FP32: 4 x 4 SIMT
+// micro-tiles per thread.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void rank_update_f64(double* A, int lda, double* V, int ldv, int n, int K, int kb,
+                                                int R0, int nv, bool factor) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int M = n - R0;
+  const int tm = (M + 15) / 16;
+  const int tnA = factor ? (M + 31) / 32 : 0, tnV = (nv + 31) / 32;
+  const int nA = tm * tnA, total = nA + tm * tnV;
+  const double* P = A + R0 * lda + K;
+  for (int tile = warp; tile < total; tile += nw) {
+    const bool isA = tile < nA;
+    const int tt = isA ? tile : tile - nA;
+    const int tn = isA ? tnA : tnV;
+    const int r0 = (tt / tn) * 16, c0 = (tt % tn) * 32;
+    if (isA && c0 > r0 + 15) continue;
+    double* C = isA ? A + R0 * lda + R0 : V + R0 * ldv;
+    const int ldc = isA ? lda : ldv;
+    const int N = isA ? M : nv;
+    double acc[2][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = r0 + 8 * i + g, c = c0 + 8 * j + 2 * t + e;
+          acc[i][j][e] = (r < M && c < N) ? C[r * ldc + c] : 0.0;
+        }
+    int ra[2], cb[4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) ra[i] = min(r0 + 8 * i + g, M - 1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cb[j] = min(c0 + 8 * j + g, N - 1);
+#pragma unroll
+    for (int k0 = 0; k0 < 8; k0 += 4) {
+      const int k = k0 + t;
+      const bool kv = k < kb;
+      const int kc = kv ? k : 0;
+      double a[2], b[4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) a[i] = kv ? -P[ra[i] * lda + kc] : 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double v = isA ? P[cb[j] * lda + kc] : V[(K + kc) * ldv + cb[j]];
+        b[j] = kv ? v : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = r0 + 8 * i + g, c = c0 + 8 * j + 2 * t + e;
+          if (r < M && c < N && (!isA || c <= r)) C[r * ldc + c] = acc[i][j][e];
+        }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void rank_update_simt(T* A, int lda, T* V, int ldv, int n, int K, int kb, int R0, int nv,
+                                                 bool factor) {
+  constexpr int BK = 8;
+  const int M = n - R0;
+  const int tm = (M + 3) / 4;
+  const int tnA = factor ? (M + 3) / 4 : 0, tnV = (nv + 3) / 4;
+  const int nA = tm * tnA, total = nA + tm * tnV;
+  const T* P = A + R0 * lda + K;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const bool isA = idx < nA;
+    const int tt = isA ? idx : idx - nA;
+    const int tn = isA ? tnA : tnV;
+    const int r0 = (tt / tn) * 4, c0 = (tt % tn) * 4;
+    if (isA && c0 > r0 + 3) continue;
+    T* C = isA ? A + R0 * lda + R0 : V + R0 * ldv;
+    const int ldc = isA ? lda : ldv;
+    const int N = isA ? M : nv;
+    T acc[4][4];
+    int ra[4], cb[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) ra[i] = min(r0 + i, M - 1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cb[j] = min(c0 + j, N - 1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = C[ra[i] * ldc + cb[j]];
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      if (k < kb) {
+        T a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = P[ra[i] * lda + k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = isA ? P[cb[j] * lda + k] : V[(K + k) * ldv + cb[j]];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(-a[i], b[j], acc[i][j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = r0 + i, c = c0 + j;
+        if (r < M && c < N && (!isA || c <= r)) C[r * ldc + c] = acc[i][j];
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // CTA: blocked right-looking Cholesky of the n x n block in A fused with the
 // solve C V = V for nv vectors (columns of V), by 8-column blocks.
 //   1. every thread loads the diagonal block into registers and (when
@@ -367,13 +493,10 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
           if (i < kb) A[(K + i) * lda + K + j] = c[i][j];
     }
     if (R0 < n) {
-      const T* P = A + R0 * lda + K;
-      if (FACTOR)
-        cta_gemm<T, false, true, true>(n - R0, n - R0, kb, P, lda, P, lda,
-                                       [&](int r, int cc, T v) { A[(R0 + r) * lda + R0 + cc] -= v; });
-      if (nv > 0)
-        cta_gemm<T, false, false>(n - R0, nv, kb, P, lda, V + K * ldv, ldv,
-                                  [&](int r, int cc, T v) { V[(R0 + r) * ldv + cc] -= v; });
+      if constexpr (sizeof(T) == 8)
+        rank_update_f64(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR);
+      else
+        rank_update_simt<T>(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR);
     }
     __syncthreads();
   }
