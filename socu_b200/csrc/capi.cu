@@ -390,8 +390,7 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     const int nrc = ceil_div(a.n, kResRows);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, smem_residual_rows_elems(a.n) * sizeof(double),
-                              st>>>(a);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, st>>>(a);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
                          st>>>(a);
@@ -415,7 +414,6 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
     const size_t srow = smem_residual_rows_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
     if (residual_uses_rows(a.n)) {
-      if (e == cudaSuccess) e = prepare(k_residual_rows<true>, srow);
       if (e == cudaSuccess) e = prepare(k_ref_init_rows, srow);
     }
     if (e != cudaSuccess) return cuda_status(e);
@@ -508,8 +506,7 @@ int capture_fallback(const RefineArgs& a, const FallbackArgs& f, cudaStream_t ca
   ra.active = f.fb;
   if (st == SOCU_OK) {
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, smem_residual_rows_elems(a.n) * sizeof(double),
-                              body>>>(ra);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, body>>>(ra);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * ceil_div(a.n, kResRows)), 256,
                          smem_residual_elems(a.n) * sizeof(double), body>>>(ra);
@@ -995,7 +992,6 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
   const size_t srow = smem_residual_rows_elems(n) * sizeof(double);
   if (residual_uses_rows(n)) {
-    if (e == cudaSuccess) e = noalloc_smem(k_residual_rows<true>, srow);
     if (e == cudaSuccess) e = noalloc_smem(k_ref_init_rows, srow);
   }
   if (e != cudaSuccess) return cuda_status(e);
@@ -1029,7 +1025,7 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
     for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
     if (rows)
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), 256, srow, st>>>(a);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, st>>>(a);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
     k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
@@ -1236,11 +1232,9 @@ int socu_block_tridiag_residual(const double* L, const double* E, const double* 
   a.L = L; a.E = E; a.b = b; a.x = const_cast<double*>(x); a.rout = r;
   a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
   const size_t sres = smem_residual_elems(d.n) * sizeof(double);
-  const size_t srow = smem_residual_rows_elems(d.n) * sizeof(double);
   if (residual_uses_rows(d.n)) {
-    e = prepare(k_residual_rows<false>, srow);
-    if (e != cudaSuccess) return cuda_status(e);
-    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), 256, srow, static_cast<cudaStream_t>(stream)>>>(a);
+    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), residual_rows_threads(d.n, d.m), 0,
+                             static_cast<cudaStream_t>(stream)>>>(a);
   } else {
     e = prepare(k_residual<false>, sres);
     if (e != cudaSuccess) return cuda_status(e);

@@ -264,65 +264,74 @@ __device__ __forceinline__ void stage_block_row(const RefineArgs& a, int bi, int
   }
 }
 
-// r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block row.
+// r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block
+// row, on FP64 tensor cores (mma.m8n8k4 .f64) with the operands read straight
+// from global memory: warp task = one 8-row x 8-column output tile, 3 blocks x
+// ceil(n/4) k-steps into six independent accumulators (block x k parity).
+// Fragment layout: a0 = A[g][t], b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}]
+// (g = lane / 4, t = lane % 4).  D_i is symmetric from its lower triangle:
+// above the diagonal the transposed element is read.  No shared memory beyond
+// the block reduction; any blockDim.x that is a multiple of 32 works.
 template <bool REFINE>
-__device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
-  const int n = a.n, m = a.m, N = a.N, ld = n + 1, ldx = kResRowCols + 1;
-  double* Ls = reinterpret_cast<double*>(smem_raw);
-  double* Em = Ls + n * ld;
-  double* Ep = Em + n * ld;
-  double* X0 = Ep + n * ld;
-  double* X1 = X0 + n * ldx;
-  double* X2 = X1 + n * ldx;
+__device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char*) {
   __shared__ double red[32];
-  stage_block_row(a, bi, i, Ls, Em, Ep);
+  const int n = a.n, m = a.m, N = a.N;
+  const long long nn = (long long)n * n;
+  const double* D = a.L + ((long long)bi * N + i) * nn;
+  const bool hasM = i > 0, hasP = i < N - 1;
+  const double* Em = a.E + ((long long)bi * a.S + (hasM ? i - 1 : 0)) * nn;
+  const double* Ep = a.E + ((long long)bi * a.S + (hasP ? i : 0)) * nn;
   const long long vi = ((long long)bi * N + i) * n * m;
+  const double* x1 = a.x + vi;
+  const double* x0 = hasM ? x1 - (long long)n * m : x1;
+  const double* x2 = hasP ? x1 + (long long)n * m : x1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int rts = (n + 7) >> 3, cts = (m + 7) >> 3;
   double rmax = 0.0, xmax = 0.0;
-  for (int c0 = 0; c0 < m; c0 += kResRowCols) {
-    const int mc = min(kResRowCols, m - c0);
-    __syncthreads();
-    async_load(X1, ldx, a.x + vi + c0, n, mc, m);
-    if (i > 0) {
-      async_load(X0, ldx, a.x + vi - (long long)n * m + c0, n, mc, m);
-    } else {
-      for (int e = threadIdx.x; e < n * ldx; e += blockDim.x) X0[e] = 0.0;
-    }
-    if (i < N - 1) {
-      async_load(X2, ldx, a.x + vi + (long long)n * m + c0, n, mc, m);
-    } else {
-      for (int e = threadIdx.x; e < n * ldx; e += blockDim.x) X2[e] = 0.0;
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    for (int o = threadIdx.x; o < n * mc; o += blockDim.x) {
-      const int r = o / mc, c = o - r * mc;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0, s5 = 0.0;
-      int k = 0;
-      for (; k + 1 < n; k += 2) {
-        const double d0 = k <= r ? Ls[r * ld + k] : Ls[k * ld + r];
-        const double d1 = k + 1 <= r ? Ls[r * ld + k + 1] : Ls[(k + 1) * ld + r];
-        s0 = fma(d0, X1[k * ldx + c], s0);
-        s3 = fma(d1, X1[(k + 1) * ldx + c], s3);
-        s1 = fma(Em[r * ld + k], X0[k * ldx + c], s1);
-        s4 = fma(Em[r * ld + k + 1], X0[(k + 1) * ldx + c], s4);
-        s2 = fma(Ep[k * ld + r], X2[k * ldx + c], s2);
-        s5 = fma(Ep[(k + 1) * ld + r], X2[(k + 1) * ldx + c], s5);
+  for (int task = warp; task < rts * cts; task += nw) {
+    const int rt = task / cts, r0 = rt * 8, c0 = (task - rt * cts) * 8;
+    const int ra = r0 + g, cb = c0 + g;
+    const bool rv = ra < n, cv = cb < m;
+    const int rr = rv ? ra : 0, cc = cv ? cb : 0;
+    double acc[6][2];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q][0] = acc[q][1] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < n; k0 += 8) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = k0 + 4 * h + t;
+        const bool kv = k < n;
+        const int kk = kv ? k : 0;
+        const bool av = rv && kv, bv = kv && cv;
+        const double dv = kk <= rr ? D[rr * n + kk] : D[kk * n + rr];
+        const double aD = av ? dv : 0.0;
+        const double aM = (av && hasM) ? Em[rr * n + kk] : 0.0;
+        const double aP = (av && hasP) ? Ep[kk * n + rr] : 0.0;
+        const double b1 = bv ? x1[kk * m + cc] : 0.0;
+        const double b0 = (bv && hasM) ? x0[kk * m + cc] : 0.0;
+        const double b2 = (bv && hasP) ? x2[kk * m + cc] : 0.0;
+        dmma_8x8x4(acc[h][0], acc[h][1], aD, b1);
+        dmma_8x8x4(acc[2 + h][0], acc[2 + h][1], aM, b0);
+        dmma_8x8x4(acc[4 + h][0], acc[4 + h][1], aP, b2);
       }
-      if (k < n) {
-        const double d0 = k <= r ? Ls[r * ld + k] : Ls[k * ld + r];
-        s0 = fma(d0, X1[k * ldx + c], s0);
-        s1 = fma(Em[r * ld + k], X0[k * ldx + c], s1);
-        s2 = fma(Ep[k * ld + r], X2[k * ldx + c], s2);
-      }
-      const long long e = vi + (long long)r * m + c0 + c;
-      const double res = a.b[e] - (((s0 + s3) + (s1 + s4)) + (s2 + s5));
-      if (REFINE) {
-        a.R32[e] = (float)res;
-        const double xv = X1[r * ldx + c];
-        rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
-        xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
-      } else {
-        a.rout[e] = res;
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int r = r0 + g, c = c0 + 2 * t + e;
+      if (r < n && c < m) {
+        const long long o = vi + (long long)r * m + c;
+        const double y = ((acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e])) + (acc[4][e] + acc[5][e]);
+        const double res = a.b[o] - y;
+        if (REFINE) {
+          a.R32[o] = (float)res;
+          const double xv = x1[(long long)r * m + c];
+          rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
+          xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
+        } else {
+          a.rout[o] = res;
+        }
       }
     }
   }
@@ -334,6 +343,12 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
       atomic_max_pos(&a.st[bi].xnorm, xm);
     }
   }
+}
+
+// threads of k_residual_rows: one warp per output tile, at most 8 warps
+__host__ __device__ inline int residual_rows_threads(int n, int m) {
+  const int tiles = ((n + 7) / 8) * ((m + 7) / 8);
+  return 32 * (tiles < 8 ? tiles : 8);
 }
 
 template <bool REFINE>
