@@ -390,7 +390,8 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     const int nrc = ceil_div(a.n, kResRows);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, st>>>(a);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
+                              smem_residual_x_elems(a.n) * sizeof(double), st>>>(a);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
                          st>>>(a);
@@ -506,7 +507,8 @@ int capture_fallback(const RefineArgs& a, const FallbackArgs& f, cudaStream_t ca
   ra.active = f.fb;
   if (st == SOCU_OK) {
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, body>>>(ra);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
+                              smem_residual_x_elems(a.n) * sizeof(double), body>>>(ra);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * ceil_div(a.n, kResRows)), 256,
                          smem_residual_elems(a.n) * sizeof(double), body>>>(ra);
@@ -1025,7 +1027,8 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
     for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
     if (rows)
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m), 0, st>>>(a);
+      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
+                              smem_residual_x_elems(a.n) * sizeof(double), st>>>(a);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
     k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
@@ -1233,7 +1236,8 @@ int socu_block_tridiag_residual(const double* L, const double* E, const double* 
   a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
   const size_t sres = smem_residual_elems(d.n) * sizeof(double);
   if (residual_uses_rows(d.n)) {
-    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), residual_rows_threads(d.n, d.m), 0,
+    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), residual_rows_threads(d.n, d.m),
+                             smem_residual_x_elems(d.n) * sizeof(double),
                              static_cast<cudaStream_t>(stream)>>>(a);
   } else {
     e = prepare(k_residual<false>, sres);

@@ -265,16 +265,24 @@ __device__ __forceinline__ void stage_block_row(const RefineArgs& a, int bi, int
 }
 
 // r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block
-// row, on FP64 tensor cores (mma.m8n8k4 .f64) with the operands read straight
-// from global memory: warp task = one 8-row x 8-column output tile, 3 blocks x
-// ceil(n/4) k-steps into six independent accumulators (block x k parity).
-// Fragment layout: a0 = A[g][t], b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}]
-// (g = lane / 4, t = lane % 4).  D_i is symmetric from its lower triangle:
-// above the diagonal the transposed element is read.  No shared memory beyond
-// the block reduction; any blockDim.x that is a multiple of 32 works.
+// row, on FP64 tensor cores (mma.m8n8k4 .f64).  Per chunk of 8 right-hand
+// sides the CTA stages x_{i-1}, x_i, x_{i+1} in shared memory (stride 12:
+// conflict-free B fragments; missing neighbours and columns as zeros); the
+// matrix fragments are read straight from global memory, each element once.
+// Warp task = one 8-row output tile: 3 blocks x ceil(n/4) k-steps into six
+// independent accumulators (block x k parity).  Fragment layout: a0 = A[g][t],
+// b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}] (g = lane / 4, t = lane % 4).
+// D_i is symmetric from its lower triangle: above the diagonal the transposed
+// element is read.  Any blockDim.x that is a multiple of 32 works.
+// Shared: 3 x n x kResXld doubles (smem_residual_x_elems; the ragged kernel's
+// buffer, sized by smem_residual_rows_elems, is larger).
+constexpr int kResXld = 12;
+__host__ __device__ inline long long smem_residual_x_elems(int n) { return 3LL * n * kResXld; }
 template <bool REFINE>
-__device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char*) {
+__device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
   __shared__ double red[32];
+  double* const xs0 = reinterpret_cast<double*>(smem_raw);
+  const int xstride = a.n * kResXld;   // x_{i-1}, x_i, x_{i+1} chunks back to back
   const int n = a.n, m = a.m, N = a.N;
   const long long nn = (long long)n * n;
   const double* D = a.L + ((long long)bi * N + i) * nn;
@@ -283,54 +291,62 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
   const double* Ep = a.E + ((long long)bi * a.S + (hasP ? i : 0)) * nn;
   const long long vi = ((long long)bi * N + i) * n * m;
   const double* x1 = a.x + vi;
-  const double* x0 = hasM ? x1 - (long long)n * m : x1;
-  const double* x2 = hasP ? x1 + (long long)n * m : x1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int rts = (n + 7) >> 3, cts = (m + 7) >> 3;
+  const int rts = (n + 7) >> 3;
   double rmax = 0.0, xmax = 0.0;
-  for (int task = warp; task < rts * cts; task += nw) {
-    const int rt = task / cts, r0 = rt * 8, c0 = (task - rt * cts) * 8;
-    const int ra = r0 + g, cb = c0 + g;
-    const bool rv = ra < n, cv = cb < m;
-    const int rr = rv ? ra : 0, cc = cv ? cb : 0;
-    double acc[6][2];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) acc[q][0] = acc[q][1] = 0.0;
-#pragma unroll 2
-    for (int k0 = 0; k0 < n; k0 += 8) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int k = k0 + 4 * h + t;
-        const bool kv = k < n;
-        const int kk = kv ? k : 0;
-        const bool av = rv && kv, bv = kv && cv;
-        const double dv = kk <= rr ? D[rr * n + kk] : D[kk * n + rr];
-        const double aD = av ? dv : 0.0;
-        const double aM = (av && hasM) ? Em[rr * n + kk] : 0.0;
-        const double aP = (av && hasP) ? Ep[kk * n + rr] : 0.0;
-        const double b1 = bv ? x1[kk * m + cc] : 0.0;
-        const double b0 = (bv && hasM) ? x0[kk * m + cc] : 0.0;
-        const double b2 = (bv && hasP) ? x2[kk * m + cc] : 0.0;
-        dmma_8x8x4(acc[h][0], acc[h][1], aD, b1);
-        dmma_8x8x4(acc[2 + h][0], acc[2 + h][1], aM, b0);
-        dmma_8x8x4(acc[4 + h][0], acc[4 + h][1], aP, b2);
-      }
+  for (int c0 = 0; c0 < m; c0 += 8) {
+    const int mc = min(8, m - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * n * 8; e += blockDim.x) {
+      const int j = e / (n * 8), rem = e - j * n * 8, k = rem >> 3, c = rem & 7;
+      const bool ok = c < mc && (j == 1 || (j == 0 ? hasM : hasP));
+      xs0[j * xstride + k * kResXld + c] = ok ? x1[(long long)(j - 1) * n * m + (long long)k * m + c0 + c] : 0.0;
     }
+    __syncthreads();
+    for (int rt = warp; rt < rts; rt += nw) {
+      const int r0 = rt * 8, ra = r0 + g;
+      const bool rv = ra < n;
+      const int rr = rv ? ra : 0;
+      double acc[6][2];
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int r = r0 + g, c = c0 + 2 * t + e;
-      if (r < n && c < m) {
-        const long long o = vi + (long long)r * m + c;
-        const double y = ((acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e])) + (acc[4][e] + acc[5][e]);
-        const double res = a.b[o] - y;
-        if (REFINE) {
-          a.R32[o] = (float)res;
-          const double xv = x1[(long long)r * m + c];
-          rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
-          xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
-        } else {
-          a.rout[o] = res;
+      for (int q = 0; q < 6; ++q) acc[q][0] = acc[q][1] = 0.0;
+#pragma unroll 2
+      for (int k0 = 0; k0 < n; k0 += 8) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k = k0 + 4 * h + t;
+          const bool kv = k < n;
+          const int kk = kv ? k : 0;
+          const bool av = rv && kv;
+          const double dv = kk <= rr ? D[rr * n + kk] : D[kk * n + rr];
+          const double aD = av ? dv : 0.0;
+          const double aM = (av && hasM) ? Em[rr * n + kk] : 0.0;
+          const double aP = (av && hasP) ? Ep[kk * n + rr] : 0.0;
+          const int xo = kk * kResXld + g;
+          const double b1 = kv ? xs0[xstride + xo] : 0.0;
+          const double b0 = kv ? xs0[xo] : 0.0;
+          const double b2 = kv ? xs0[2 * xstride + xo] : 0.0;
+          dmma_8x8x4(acc[h][0], acc[h][1], aD, b1);
+          dmma_8x8x4(acc[2 + h][0], acc[2 + h][1], aM, b0);
+          dmma_8x8x4(acc[4 + h][0], acc[4 + h][1], aP, b2);
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = r0 + g, c = 2 * t + e;
+        if (r < n && c < mc) {
+          const long long o = vi + (long long)r * m + c0 + c;
+          const double y = ((acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e])) + (acc[4][e] + acc[5][e]);
+          const double res = a.b[o] - y;
+          if (REFINE) {
+            a.R32[o] = (float)res;
+            const double xv = xs0[xstride + r * kResXld + c];
+            rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
+            xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
+          } else {
+            a.rout[o] = res;
+          }
         }
       }
     }
@@ -345,14 +361,11 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
   }
 }
 
-// threads of k_residual_rows: one warp per output tile, at most 8 warps
-__host__ __device__ inline int residual_rows_threads(int n, int m) {
-  const int tiles = ((n + 7) / 8) * ((m + 7) / 8);
-  return 32 * (tiles < 8 ? tiles : 8);
-}
+// threads of k_residual_rows: one warp per 8-row tile
+__host__ __device__ inline int residual_rows_threads(int n, int) { return 32 * ((n + 7) / 8); }
 
 template <bool REFINE>
-__global__ void __launch_bounds__(256) k_residual_rows(RefineArgs a) {
+__global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
   const int bi = blockIdx.x / a.N;
   const int i = blockIdx.x - bi * a.N;
   if (REFINE && !a.active[bi]) return;
