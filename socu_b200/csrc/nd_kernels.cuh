@@ -485,9 +485,13 @@ __device__ void sweep_upper_solve(T* Y, int ldy, int mc, const T* __restrict__ L
 // vector leading dimension of the resident sweeps: rows start on 16 bytes and
 // every 8-column pass can read 8 elements past its first column
 __host__ __device__ inline int res_ldy(int mc) { return ((mc + 3) / 4) * 4 + 4; }
+// block leading dimension of the resident sweeps: rows start on 16 bytes (one
+// 16-byte copy per 4 floats / 2 doubles) and 4 threads x 8 rows of a warp hit
+// distinct banks in the row-major reads
+__host__ __device__ inline int res_ldm(int n) { return ((n + 3) & ~3) + 4; }
 __host__ __device__ inline long long smem_sweep_res_elems(int n, int m) {
   const int mc = min_i(m, kMC);
-  return 3LL * n * even_ld(n) + 3LL * n * res_ldy(mc) + n;
+  return 3LL * n * res_ldm(n) + 3LL * n * res_ldy(mc) + n;
 }
 
 // CW consecutive elements from 16-byte-aligned shared memory (8-byte for CW = 2 floats)
@@ -536,6 +540,7 @@ __device__ __forceinline__ void res_rowdot(T* Yout, const T* Z, int ldy, int mc,
 #pragma unroll
       for (int j = 0; j < CW; ++j) acc[j] = T(0);
       const int k0 = MODE == 2 ? r + 1 : 0, k1 = MODE == 3 ? r : n;
+#pragma unroll 4
       for (int k = k0 + q; k < k1; k += 4) {
         const T mv = (MODE == 0 || MODE == 2) ? M[r * ldm + k] : M[k * ldm + r];
         T z[CW];
@@ -560,6 +565,67 @@ __device__ __forceinline__ void res_rowdot(T* Yout, const T* Z, int ldy, int mc,
       }
     }
   }
+}
+
+// Both coupling products of a sweep node in one pass:
+//   Y -= A1 Z1 + A2 Z2,   A(r,k) = M[k*ldm + r] if transposed else M[r*ldm + k];
+// a null M skips its product.  Same thread layout as res_rowdot.
+template <typename T, int CW, bool TR1, bool TR2>
+__device__ __forceinline__ void res_rowdot_pair(T* Y, const T* Z1, const T* M1, const T* Z2, const T* M2, int ldy,
+                                                int mc, int ldm, int n) {
+  const int q = threadIdx.x & 3;
+  const int nr = ((n + 7) / 8) * 8;
+  const bool h1 = M1 != nullptr, h2 = M2 != nullptr;
+  for (int c0 = 0; c0 < mc; c0 += CW) {
+    for (int rb = threadIdx.x >> 2; rb < nr; rb += blockDim.x >> 2) {
+      const int r = rb < n ? rb : n - 1;
+      T acc[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) acc[j] = T(0);
+#pragma unroll 4
+      for (int k = q; k < n; k += 4) {
+        if (h1) {
+          const T mv = TR1 ? M1[k * ldm + r] : M1[r * ldm + k];
+          T z[CW];
+          load_cols<T, CW>(Z1 + k * ldy + c0, z);
+#pragma unroll
+          for (int j = 0; j < CW; ++j) acc[j] = fma(mv, z[j], acc[j]);
+        }
+        if (h2) {
+          const T mv = TR2 ? M2[k * ldm + r] : M2[r * ldm + k];
+          T z[CW];
+          load_cols<T, CW>(Z2 + k * ldy + c0, z);
+#pragma unroll
+          for (int j = 0; j < CW; ++j) acc[j] = fma(mv, z[j], acc[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        acc[j] += __shfl_xor_sync(kFull, acc[j], 1);
+        acc[j] += __shfl_xor_sync(kFull, acc[j], 2);
+      }
+      if (rb < n) {
+#pragma unroll
+        for (int j = 0; j < CW; ++j) {
+          if ((j & 3) != q || c0 + j >= mc) continue;
+          Y[r * ldy + c0 + j] -= acc[j];
+        }
+      }
+    }
+  }
+}
+
+template <typename T, bool TR1, bool TR2>
+__device__ __forceinline__ void res_matvec_pair(T* Y, const T* Z1, const T* M1, const T* Z2, const T* M2, int ldy,
+                                                int mc, int ldm, int n) {
+  if (mc >= 8)
+    res_rowdot_pair<T, 8, TR1, TR2>(Y, Z1, M1, Z2, M2, ldy, mc, ldm, n);
+  else if (mc >= 4)
+    res_rowdot_pair<T, 4, TR1, TR2>(Y, Z1, M1, Z2, M2, ldy, mc, ldm, n);
+  else if (mc >= 2)
+    res_rowdot_pair<T, 2, TR1, TR2>(Y, Z1, M1, Z2, M2, ldy, mc, ldm, n);
+  else
+    res_rowdot_pair<T, 1, TR1, TR2>(Y, Z1, M1, Z2, M2, ldy, mc, ldm, n);
 }
 
 template <typename T, int MODE>
@@ -670,7 +736,7 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
   T* Ms = Z2 + n * ldy;   // RES: C, F, G (n x ldm each), dv (n); else Cc (n x (kTile+1)), dv
-  const int ldm = even_ld(n);
+  const int ldm = res_ldm(n);
   T* Cs = Ms;
   T* Fs = Cs + n * ldm;
   T* Gs = Fs + n * ldm;
@@ -693,11 +759,8 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
     if (RES) {
       if (c0 == 0 && solve)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
-      if (pull) {
-        res_matvec<T, 0>(Y, Z1, ldy, mc, Fs, ldm, nullptr, n);          // Y -= F y_{j-h}
-        __syncthreads();
-        if (G) res_matvec<T, 1>(Y, Z2, ldy, mc, Gs, ldm, nullptr, n);   // Y -= G^T y_{j+h}
-      }
+      // Y -= F y_{j-h} + G^T y_{j+h}
+      if (pull) res_matvec_pair<T, false, true>(Y, Z1, Fs, G ? Z2 : nullptr, G ? Gs : nullptr, ldy, mc, ldm, n);
       __syncthreads();
       if (solve) {
         if (INV) {
@@ -742,7 +805,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
   T* Ms = Z2 + n * ldy;
-  const int ldm = even_ld(n);
+  const int ldm = res_ldm(n);
   T* Cs = Ms;
   T* Fs = Cs + n * ldm;
   T* Gs = Fs + n * ldm;
@@ -768,9 +831,10 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
     if (RES) {
       if (c0 == 0)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
-      if (right) res_matvec<T, 1>(Y, Z1, ldy, mc, Fs, ldm, nullptr, n);   // Y -= F^T x_{i+s}
-      __syncthreads();
-      if (left) res_matvec<T, 0>(Y, Z2, ldy, mc, Gs, ldm, nullptr, n);    // Y -= G x_{i-s}
+      // Y -= F^T x_{i+s} + G x_{i-s}
+      if (right || left)
+        res_matvec_pair<T, true, false>(Y, right ? Z1 : nullptr, right ? Fs : nullptr, left ? Z2 : nullptr,
+                                        left ? Gs : nullptr, ldy, mc, ldm, n);
       __syncthreads();
       if (INV) {
         res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
