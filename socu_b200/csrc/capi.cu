@@ -412,16 +412,13 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
-    const size_t srow = smem_residual_rows_elems(a.n) * sizeof(double);
+    const size_t sinit = smem_ref_init_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
-    if (residual_uses_rows(a.n)) {
-      if (e == cudaSuccess) e = prepare(k_ref_init_rows, srow);
-    }
     if (e != cudaSuccess) return cuda_status(e);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
     const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
     if (residual_uses_rows(a.n))
-      k_ref_init_rows<<<init_blocks, 256, srow, st>>>(a);
+      k_ref_init_rows<<<init_blocks, 256, sinit, st>>>(a);
     else
       k_ref_init<<<init_blocks, 256, 0, st>>>(a);
     e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);   // the first test decides
@@ -992,10 +989,7 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   if (e == cudaSuccess) e = noalloc_smem(pull, ss);
   if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
   if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
-  const size_t srow = smem_residual_rows_elems(n) * sizeof(double);
-  if (residual_uses_rows(n)) {
-    if (e == cudaSuccess) e = noalloc_smem(k_ref_init_rows, srow);
-  }
+  const size_t sinit = smem_ref_init_elems(n) * sizeof(double);
   if (e != cudaSuccess) return cuda_status(e);
   (void)0;
   const int nrc = ceil_div(n, kResRows);
@@ -1008,7 +1002,7 @@ int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
   const bool rows = residual_uses_rows(n);
   const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
   if (rows)
-    k_ref_init_rows<<<init_blocks, 256, srow, st>>>(a);
+    k_ref_init_rows<<<init_blocks, 256, sinit, st>>>(a);
   else
     k_ref_init<<<init_blocks, 256, 0, st>>>(a);
   // first round fused into the float factor: factor_and_solve of R32 = b

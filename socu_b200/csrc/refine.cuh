@@ -375,10 +375,17 @@ __global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
 
 // Refinement set-up for block row i (if i < N) and storage slot i (if i < S):
 // float copies of L_i and slot i, R32 = b_i, x_i = 0, ||b||_inf and the row
-// sums of |Psi| over block row i, all from shared memory.
+// sums of |Psi| over block row i.  One streaming pass, no staging: warp w
+// takes rows w, w + nw, ... of L_i, E_{i-1} and E_i with coalesced loads
+// (lane owns columns lane and lane + 32), writes the float copies, reduces
+// the row part of each row sum (lower(D) row, E_{i-1} row) with shuffles and
+// keeps per-lane column partials for the transposed parts (strict lower(D)
+// columns, E_i columns).  The warps' column partials are added in warp order
+// in shared memory (smem_ref_init_elems doubles), so the sums are deterministic.
+__host__ __device__ inline long long smem_ref_init_elems(int n) { return 2LL * 8 * n + n; }
 __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
   __shared__ double red[32];
-  const int n = a.n, m = a.m, N = a.N, ld = n + 1;
+  const int n = a.n, m = a.m, N = a.N;
   const long long nn = (long long)n * n;
   if (i >= N) {   // storage tail: zero slots only
     if (i < a.S) {
@@ -387,10 +394,15 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
     }
     return;
   }
-  double* Ls = reinterpret_cast<double*>(smem_raw);
-  double* Em = Ls + n * ld;
-  double* Ep = Em + n * ld;
-  stage_block_row(a, bi, i, Ls, Em, Ep);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* colp = reinterpret_cast<double*>(smem_raw);   // [warp][2][n] column partials
+  double* rs = colp + 2 * 8 * n;                         // [n] row parts
+  const bool hasM = i > 0, hasP = i < N - 1, hasS = i < a.S;
+  const double* Lg = a.L + ((long long)bi * N + i) * nn;
+  const double* Em = a.E + ((long long)bi * a.S + (hasM ? i - 1 : 0)) * nn;
+  const double* Ep = a.E + ((long long)bi * a.S + (hasP ? i : 0)) * nn;
+  float* L32 = a.L32 + ((long long)bi * N + i) * nn;
+  float* E32 = a.E32 + ((long long)bi * a.S + (hasS ? i : 0)) * nn;
   const long long vo = ((long long)bi * N + i) * n * m;
   double bmax = 0.0;
   for (int e = threadIdx.x; e < n * m; e += blockDim.x) {
@@ -399,25 +411,47 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
     a.x[vo + e] = 0.0;
     bmax = fmax(bmax, fabs(v));
   }
-  cp_async_wait_all();
-  __syncthreads();
-  float* L32 = a.L32 + ((long long)bi * N + i) * nn;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) L32[e] = (float)Ls[(e / n) * ld + e % n];
-  if (i < a.S) {
-    float* E32 = a.E32 + ((long long)bi * a.S + i) * nn;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) E32[e] = (float)Ep[(e / n) * ld + e % n];
+  double cl[2] = {0.0, 0.0}, ce[2] = {0.0, 0.0};
+  for (int r = warp; r < n; r += nw) {
+    double vl[2], vm[2], vp[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      const bool ok = c < n;
+      const int o = r * n + (ok ? c : 0);
+      vl[h] = ok ? Lg[o] : 0.0;
+      vm[h] = (ok && hasM) ? Em[o] : 0.0;
+      vp[h] = (ok && hasP) ? Ep[o] : 0.0;
+    }
+    double part = 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      if (c < n) {
+        L32[r * n + c] = (float)vl[h];
+        if (hasS) E32[r * n + c] = (float)vp[h];
+        part += (c <= r ? fabs(vl[h]) : 0.0) + fabs(vm[h]);
+        cl[h] += c < r ? fabs(vl[h]) : 0.0;   // D(c, r) = L[r][c] for r > c: row c's transposed part
+        ce[h] += fabs(vp[h]);                 // E_i^T couples row c to x_{i+1}: column sums of E_i
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    if (lane == 0) rs[r] = part;
   }
-  // row r: four threads per row, strided columns, combined by shuffles
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c = lane + 32 * h;
+    if (c < n) {
+      colp[(warp * 2 + 0) * n + c] = cl[h];
+      colp[(warp * 2 + 1) * n + c] = ce[h];
+    }
+  }
+  __syncthreads();
   double rmax = 0.0;
-  const int q = threadIdx.x & 3;
-  for (int r0 = threadIdx.x >> 2; r0 < ((n + 7) / 8) * 8; r0 += blockDim.x >> 2) {
-    const int r = r0 < n ? r0 : n - 1;
-    double sum = 0.0;
-    for (int c = q; c < n; c += 4)
-      sum += fabs(c <= r ? Ls[r * ld + c] : Ls[c * ld + r]) + fabs(Em[r * ld + c]) + fabs(Ep[c * ld + r]);
-    sum += __shfl_xor_sync(kFull, sum, 1);
-    sum += __shfl_xor_sync(kFull, sum, 2);
-    if (r0 < n) rmax = fmax(rmax, sum);
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double sum = rs[r];
+    for (int w = 0; w < nw; ++w) sum += colp[(w * 2 + 0) * n + r] + colp[(w * 2 + 1) * n + r];
+    rmax = fmax(rmax, sum);
   }
   const double bm = block_max(bmax, red);
   const double pm = block_max(rmax, red);
