@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <new>
 #include <utility>
@@ -79,6 +80,39 @@ cudaError_t prepare(K kernel, size_t smem) {
   const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) g_prepared[key] = smem;
   return e;
+}
+
+// Threads per CTA for a node launch: 128 instead of 256 when the narrower
+// CTAs (twice as many resident per SM) finish the level in fewer waves, as on
+// the wide bottom level of the float factor (measured: 80 -> 70 us for 512
+// n = 64 nodes; the Schur-update launches lose more per CTA than the waves
+// save and keep 256).  Occupancies are cached per kernel, device and
+// shared-memory size.
+std::mutex g_occ_mu;
+std::map<std::tuple<const void*, int, size_t, int>, int> g_occ;
+
+template <typename K>
+int level_threads(K kernel, int nth, long long blocks, size_t smem) {
+  if (nth != 256 || blocks <= 0) return nth;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+    return nth;
+  auto occ = [&](int threads) {
+    const auto key = std::make_tuple(reinterpret_cast<const void*>(kernel), dev, smem, threads);
+    std::lock_guard<std::mutex> g(g_occ_mu);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) return it->second;
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess) v = 0;
+    g_occ[key] = v;
+    return v;
+  };
+  const int o256 = occ(256), o128 = occ(128);
+  if (o256 <= 0 || o128 <= 0) return nth;
+  const long long w256 = (blocks + (long long)sms * o256 - 1) / ((long long)sms * o256);
+  const long long w128 = (blocks + (long long)sms * o128 - 1) / ((long long)sms * o128);
+  return w128 < w256 ? 128 : 256;
 }
 
 // The library links the CUDA runtime statically, so its notion of the
@@ -193,6 +227,9 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     ++launches;
     if (run) kernel<<<(unsigned)blocks, threads > 0 ? threads : nth, smem, s>>>(p, L);
   };
+  auto wide = [&](auto kernel, long long blocks, size_t smem) {
+    return run ? level_threads(kernel, nth, blocks, smem) : nth;
+  };
   auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
     go_on(st, kernel, blocks, smem, L, threads);
   };
@@ -202,7 +239,8 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   if (factor) {
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
-      go(node_kernel, (long long)p.B * L.d, sd, L, nth);
+      const long long node_blocks = (long long)p.B * L.d;
+      go(node_kernel, node_blocks, sd, L, wide(node_kernel, node_blocks, sd));
       if (l + 1 < K) {
         // fused forward: apply this level's updates to every target vector
         const long long pull_blocks = withY ? (long long)p.B * (p.N / lv[l + 1].s) : 0;
