@@ -641,6 +641,91 @@ __device__ __forceinline__ void res_matvec(T* Yout, const T* Z, int ldy, int mc,
     res_rowdot<T, MODE, 1>(Yout, Z, ldy, mc, M, ldm, dv, n);
 }
 
+// ---------------------------------------------------------------------------
+// Products of the resident inverse sweeps on FP64 tensor cores (mma.m8n8k4
+// .f64), for float and double blocks: operands are widened to double in
+// registers, so products are exact and sums are FP64; the result is rounded
+// to T once.  A(r,k) = TR ? M[k*ld + r] : M[r*ld + k].
+//   MODE 0: Out -= A1 Z1 + A2 Z2     (a null A skips its product)
+//   MODE 2: Out  = dv .* Z1 + A1 Z1, A1 strictly upper (k > r)
+//   MODE 3: Out  = dv .* Z1 + A1 Z1, A1 strictly lower (k < r)
+// Out never aliases Z1 or Z2.  Warp task = one 8 x 8 output tile, all k-steps,
+// two accumulators per product (alternate k-steps).  Fragment layout: a0 =
+// A[g][t], b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}] (g = lane / 4, t = lane % 4).
+// ---------------------------------------------------------------------------
+// FP64 sweeps always take the tensor-core products (faster at every level);
+// FP32 sweeps only in launches of more than three CTAs per SM (more than one
+// wave of resident sweep CTAs), which are throughput-bound (measured at
+// N=1024, n=64: bottom level 17.0 -> 15.7 us), while the dependent DMMA chain
+// costs ~0.6 us per node on the 1-256-CTA levels and in the persistent ragged
+// CTAs, where the SIMT products are faster.
+template <typename T>
+__device__ __forceinline__ bool sweep_uses_dmma() {
+  if (sizeof(T) == 8) return true;
+  unsigned nsm;
+  asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+  return gridDim.x > 3 * nsm;
+}
+
+template <typename T, int MODE, bool TR>
+__device__ __forceinline__ double dmma_a(const T* A, int ld, int n, int r, int k) {
+  bool ok = r < n && k < n;
+  if (MODE == 2) ok = ok && k > r;
+  if (MODE == 3) ok = ok && k < r;
+  const int rr = r < n ? r : 0, kk = k < n ? k : 0;
+  const T v = TR ? A[kk * ld + rr] : A[rr * ld + kk];
+  return ok ? (double)v : 0.0;
+}
+
+template <typename T, int MODE, bool TR1, bool TR2>
+__device__ void dmma_product(T* Out, const T* Z1, const T* A1, int ld1, const T* Z2, const T* A2, int ld2, int ldy,
+                             int mc, const T* dv, int n) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int rt = (n + 7) >> 3, ct = (mc + 7) >> 3, kt = (n + 3) >> 2;
+  const bool h1 = A1 != nullptr, h2 = MODE == 0 && A2 != nullptr;
+  for (int task = warp; task < rt * ct; task += nw) {
+    const int r0 = (task / ct) * 8, c0 = (task % ct) * 8;
+    const int ra = r0 + g, cb = c0 + g;
+    const bool cv = cb < mc;
+    const int cc = cv ? cb : 0;
+    double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    int kb0 = 0, kb1 = kt;
+    if (MODE == 2) kb0 = (r0 + 1) >> 2;                             // first k-step with some k > r
+    if (MODE == 3) kb1 = min_i(kt, (r0 + 7 + 3) >> 2);              // past the last with some k < r
+    for (int kb = kb0; kb < kb1; kb += 2) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {   // two k-steps, one accumulator each
+        const int k = (kb + h) * 4 + t;
+        const bool kv = kb + h < kb1 && k < n;
+        const int kk = kv ? k : 0;
+        if (h1) {
+          const double a = kv ? dmma_a<T, MODE, TR1>(A1, ld1, n, ra, kk) : 0.0;
+          const double b = (kv && cv) ? (double)Z1[kk * ldy + cc] : 0.0;
+          dmma_8x8x4(acc[h][0], acc[h][1], a, b);
+        }
+        if (h2) {
+          const double a = kv ? dmma_a<T, MODE, TR2>(A2, ld2, n, ra, kk) : 0.0;
+          const double b = (kv && cv) ? (double)Z2[kk * ldy + cc] : 0.0;
+          dmma_8x8x4(acc[2 + h][0], acc[2 + h][1], a, b);
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int r = r0 + g, c = c0 + 2 * t + e;
+      if (r < n && c < mc) {
+        const double v = (acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]);
+        T* out = Out + r * ldy + c;
+        if (MODE == 0)
+          *out = (T)((double)*out - v);
+        else
+          *out = (T)((double)dv[r] * (double)Z1[r * ldy + c] + v);
+      }
+    }
+  }
+}
+
 // Y <- C^{-1} Y (UPPER: Y <- C^{-T} Y), C = lower(Cs) resident, dv[r] = 1/C[r][r].
 // Right-looking by 8-row blocks: one thread per column solves the block
 // against the 8x8 diagonal block held in registers, then every (row, column)
@@ -760,11 +845,20 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
       if (c0 == 0 && solve)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
       // Y -= F y_{j-h} + G^T y_{j+h}
-      if (pull) res_matvec_pair<T, false, true>(Y, Z1, Fs, G ? Z2 : nullptr, G ? Gs : nullptr, ldy, mc, ldm, n);
+      const bool tc = INV && sweep_uses_dmma<T>();
+      if (pull) {
+        if (tc)
+          dmma_product<T, 0, false, true>(Y, Z1, Fs, ldm, G ? Z2 : nullptr, G ? Gs : nullptr, ldm, ldy, mc, nullptr, n);
+        else
+          res_matvec_pair<T, false, true>(Y, Z1, Fs, G ? Z2 : nullptr, G ? Gs : nullptr, ldy, mc, ldm, n);
+      }
       __syncthreads();
       if (solve) {
         if (INV) {
-          res_matvec<T, 3>(Z2, Y, ldy, mc, Cs, ldm, dv, n);
+          if (tc)
+            dmma_product<T, 3, true, false>(Z2, Y, Cs, ldm, nullptr, nullptr, 0, ldy, mc, dv, n);   // y = W Y
+          else
+            res_matvec<T, 3>(Z2, Y, ldy, mc, Cs, ldm, dv, n);
           __syncthreads();
           store_block(yj + c0, p.m, Z2, ldy, n, mc);
           continue;
@@ -832,12 +926,21 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
       if (c0 == 0)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
       // Y -= F^T x_{i+s} + G x_{i-s}
-      if (right || left)
-        res_matvec_pair<T, true, false>(Y, right ? Z1 : nullptr, right ? Fs : nullptr, left ? Z2 : nullptr,
-                                        left ? Gs : nullptr, ldy, mc, ldm, n);
+      const bool tc = INV && sweep_uses_dmma<T>();
+      if (right || left) {
+        if (tc)
+          dmma_product<T, 0, true, false>(Y, right ? Z1 : nullptr, right ? Fs : nullptr, ldm, left ? Z2 : nullptr,
+                                          left ? Gs : nullptr, ldm, ldy, mc, nullptr, n);
+        else
+          res_matvec_pair<T, true, false>(Y, right ? Z1 : nullptr, right ? Fs : nullptr, left ? Z2 : nullptr,
+                                          left ? Gs : nullptr, ldy, mc, ldm, n);
+      }
       __syncthreads();
       if (INV) {
-        res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
+        if (tc)
+          dmma_product<T, 2, false, false>(Z1, Y, Cs, ldm, nullptr, nullptr, 0, ldy, mc, dv, n);   // x = W^T Y
+        else
+          res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
         __syncthreads();
         store_block(xi + c0, p.m, Z1, ldy, n, mc);
         continue;
