@@ -200,8 +200,10 @@ __device__ __forceinline__ void smem_gemm(int M, int N, int K, const T* __restri
 }
 
 // ---------------------------------------------------------------------------
-// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) warp GEMM on shared operands.
-//   acc(r,c) = sum_{k<K} opA(r,k) opB(k,c);  out(r, c, acc) per valid entry.
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) warp GEMM on shared operands
+// of type T (float operands are widened to double in registers: exact
+// products, FP64 sums).
+//   acc(r,c) = sum_{k<K} opA(r,k) opB(k,c);  out(r, c, acc) per valid entry, acc a double.
 // Warp tiles of 16 x 32 (2 x 4 mma tiles).  Fragment layouts (PTX ISA,
 // mma.m8n8k4 .f64): A a0 = A[g][t], B b0 = B[t][g], C {c0,c1} = C[g][2t+{0,1}]
 // with g = lane/4, t = lane%4.  Leading dimensions of 4 (mod 16) doubles make
@@ -215,9 +217,9 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 
 __host__ __device__ inline int ld_dmma(int n) { return ((n + 15) / 16) * 16 + 4; }
 
-template <bool TA, bool TB, bool LOWER = false, class Out>
-__device__ __forceinline__ void warp_gemm_f64(int M, int N, int K, const double* __restrict__ A, int lda,
-                                              const double* __restrict__ B, int ldb, Out out) {
+template <typename T, bool TA, bool TB, bool LOWER = false, class Out>
+__device__ __forceinline__ void warp_gemm_dmma(int M, int N, int K, const T* __restrict__ A, int lda,
+                                               const T* __restrict__ B, int ldb, Out out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int tm = (M + 15) / 16, tn = (N + 31) / 32;
@@ -242,12 +244,12 @@ __device__ __forceinline__ void warp_gemm_f64(int M, int N, int K, const double*
       double a[2], b[4];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
-        const double v = TA ? A[kc * lda + ra[i]] : A[ra[i] * lda + kc];
+        const double v = (double)(TA ? A[kc * lda + ra[i]] : A[ra[i] * lda + kc]);
         a[i] = kv ? v : 0.0;
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const double v = TB ? B[cb[j] * ldb + kc] : B[kc * ldb + cb[j]];
+        const double v = (double)(TB ? B[cb[j] * ldb + kc] : B[kc * ldb + cb[j]]);
         b[j] = kv ? v : 0.0;
       }
 #pragma unroll
@@ -272,7 +274,7 @@ template <typename T, bool TA, bool TB, bool LOWER = false, class Out>
 __device__ __forceinline__ void cta_gemm(int M, int N, int K, const T* __restrict__ A, int lda,
                                          const T* __restrict__ B, int ldb, Out out) {
   if constexpr (sizeof(T) == 8)
-    warp_gemm_f64<TA, TB, LOWER>(M, N, K, A, lda, B, ldb, out);
+    warp_gemm_dmma<double, TA, TB, LOWER>(M, N, K, A, lda, B, ldb, out);
   else
     smem_gemm<T, 4, 4, TA, TB, LOWER>(M, N, K, A, lda, B, ldb, out);
 }

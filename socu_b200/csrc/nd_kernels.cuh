@@ -311,9 +311,12 @@ __device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv
 // j = 2su-1 completely (all lower tiles, K = 2n), task U + t-1 forms the whole
 // fill-in block of node t.  One CTA per block keeps every warp busy.
 __host__ __device__ inline int update_blocks(int N, const Level& lv) { return N / (2 * lv.s) + lv.d - 1; }
+// n <= 64 updates run on DMMA for both types; float rows padded to 4 (mod 32)
+// words so the fragment loads hit distinct banks
+__host__ __device__ inline int update_full_ld(int k, int es) { return es == 8 ? update_ld(k, es) : ((k + 3) & ~3) + 4; }
 __host__ __device__ inline long long smem_update_full_elems(int n, int es) {
-  const long long a = (long long)n * update_ld(2 * n, es);
-  const long long f = 2LL * n * update_ld(n, es);
+  const long long a = (long long)n * update_full_ld(2 * n, es);
+  const long long f = 2LL * n * update_full_ld(n, es);
   return a > f ? a : f;
 }
 
@@ -331,15 +334,18 @@ __device__ __forceinline__ void update_full_body(const Problem<T>& p, const Leve
     const bool hasG = j + s < N;
     const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
     const int K = hasG ? 2 * n : n;
-    const int lda = update_ld(2 * n, es);
+    const int lda = update_full_ld(2 * n, es);
     // Ab[r][k] = F[r][k], Ab[r][n+k] = G[k][r]
     async_load(Ab, lda, F, n, n, n);
     if (hasG) async_load_t(Ab + n, lda, G, n, n, n);
     cp_async_wait_all();
     __syncthreads();
     T* Lj = p.Lb(b, j);
-    cta_gemm<T, false, true, true>(n, n, K, Ab, lda, Ab, lda,
-                                   [&](int r, int c, T v) { Lj[(long long)r * n + c] -= v; });
+    // DMMA for both types (float operands widened: one rounding per entry)
+    warp_gemm_dmma<T, false, true, true>(n, n, K, Ab, lda, Ab, lda, [&](int r, int c, double v) {
+      T* o = Lj + (long long)r * n + c;
+      *o = (T)((double)*o - v);
+    });
   } else {
     const int t = task - U + 1;
     const int i = s - 1 + 2 * s * t;
@@ -347,14 +353,16 @@ __device__ __forceinline__ void update_full_body(const Problem<T>& p, const Leve
     const T* F = p.Eb(b, lv.oc + 2 * t);
     const T* G = p.Eb(b, lv.oc + 2 * t - 1);
     T* X = p.Eb(b, lv.on + t - 1);
-    const int ld = update_ld(n, es);
+    const int ld = update_full_ld(n, es);
     T* Bb = Ab + n * ld;
     async_load(Ab, ld, F, n, n, n);
     async_load(Bb, ld, G, n, n, n);
     cp_async_wait_all();
     __syncthreads();
-    cta_gemm<T, false, false>(n, n, n, Ab, ld, Bb, ld,
-                              [&](int r, int c, T v) { X[(long long)r * n + c] -= v; });
+    warp_gemm_dmma<T, false, false>(n, n, n, Ab, ld, Bb, ld, [&](int r, int c, double v) {
+      T* o = X + (long long)r * n + c;
+      *o = (T)((double)*o - v);
+    });
   }
 }
 
