@@ -42,7 +42,7 @@ RAGGED_COUNT, RAGGED_SEED = 4096, 0
 # DRAM bytes (read + write) per k_bwd<float, resident, inverse> launch, averaged
 # over one backward sweep of this workload, from the ncu capture summarised in
 # profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md
-TRAFFIC_BYTES = 4999796
+TRAFFIC_BYTES = 5005218
 TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md"
 RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
                    "instance i seeded with 0 + i, one persistent launch per solve")
