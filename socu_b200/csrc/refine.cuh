@@ -234,35 +234,16 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Block-row kernels for n <= kResRowMaxN: one CTA per block row i stages the
-// three blocks of that row, L_i, E_{i-1} and E_i, in shared memory with
-// coalesced loads (missing neighbours as zeros), so every element of L and E
-// is read from HBM once per row that needs it and never column-wise.
-// Shared: Ls, Em, Ep (n x (n+1) each), X0, X1, X2 (n x (kResRowCols+1)).
+// Block-row kernels for n <= kResRowMaxN: one CTA per block row i reads the
+// three blocks of that row, L_i, E_{i-1} and E_i, with coalesced loads
+// (missing neighbours as zeros), so every element of L and E is read from HBM
+// once per row that needs it.  smem_residual_rows_elems is the shared memory
+// the ragged kernel reserves for these bodies (its persistent grid is sized
+// with it); they use less (smem_ref_init_elems, smem_residual_x_elems).
 // ---------------------------------------------------------------------------
 constexpr int kResRowMaxN = 64;
-constexpr int kResRowCols = 8;
-__host__ __device__ inline long long smem_residual_rows_elems(int n) {
-  return 3LL * n * (n + 1) + 3LL * n * (kResRowCols + 1);
-}
+__host__ __device__ inline long long smem_residual_rows_elems(int n) { return 3LL * n * (n + 1) + 27LL * n; }
 __host__ __device__ inline bool residual_uses_rows(int n) { return n <= kResRowMaxN; }
-
-__device__ __forceinline__ void stage_block_row(const RefineArgs& a, int bi, int i, double* Ls, double* Em,
-                                                double* Ep) {
-  const int n = a.n, N = a.N, ld = n + 1;
-  const long long nn = (long long)n * n;
-  async_load(Ls, ld, a.L + ((long long)bi * N + i) * nn, n, n, n);
-  if (i > 0) {
-    async_load(Em, ld, a.E + ((long long)bi * a.S + i - 1) * nn, n, n, n);
-  } else {
-    for (int e = threadIdx.x; e < n * ld; e += blockDim.x) Em[e] = 0.0;
-  }
-  if (i < N - 1) {
-    async_load(Ep, ld, a.E + ((long long)bi * a.S + i) * nn, n, n, n);
-  } else {
-    for (int e = threadIdx.x; e < n * ld; e += blockDim.x) Ep[e] = 0.0;
-  }
-}
 
 // r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block
 // row, on FP64 tensor cores (mma.m8n8k4 .f64).  Per chunk of 8 right-hand
