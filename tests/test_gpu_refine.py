@@ -14,7 +14,8 @@ def t(a):
     return torch.tensor(a, dtype=torch.float64, device=DEV)
 
 
-@pytest.mark.parametrize("N,n,m", [(1, 8, 1), (7, 10, 2), (64, 32, 4), (100, 36, 1), (33, 64, 8), (9, 128, 3)])
+@pytest.mark.parametrize("N,n,m", [(1, 8, 1), (7, 10, 2), (64, 32, 4), (100, 36, 1), (33, 64, 8), (9, 128, 3),
+                                   (20, 13, 11), (5, 64, 17), (3, 1, 9), (2, 7, 8)])
 def test_residual_matches_oracle(N, n, m):
     L, E, b = generators.readme_problem(N, n, m, shift=10.0, seed=N + n)
     x = np.random.default_rng(1).standard_normal(b.shape)
