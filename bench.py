@@ -20,6 +20,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -97,7 +98,9 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_{os.getpid()}.csv")
+        # raw samples (the summary goes into the JSON line); SOCU_BENCH_CLOCKS_DIR keeps them elsewhere
+        out_dir = os.environ.get("SOCU_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
