@@ -119,6 +119,65 @@ int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L
 
 int socu_launch_run(socu_launch_t launch, void* stream);
 
+/* ---- launch settings and autotuning (no counterpart in the reference, whose
+ * launches take block_dim / block_size per call,
+ * socu/block_tridiag_solver.py:739-747, 776-781) ----
+ * Every field 0 = not set (built-in heuristic).  node/update/sweep_threads:
+ * threads per CTA of the node, Schur-update and sweep kernels (64, 128 or
+ * 256).  sweep_tensor_cores: float sweeps on inverse-carrying factors use FP64
+ * tensor-core (1) or SIMT (2) products.  update_tile: output tile of the
+ * blocked Schur update for n > 64 (16 or 32; the reference's block_size).
+ * ragged_units: level nodes per task chunk of a ragged batch (1..64). */
+typedef struct socu_tuning {
+  int32_t node_threads;
+  int32_t update_threads;
+  int32_t sweep_threads;
+  int32_t sweep_tensor_cores;
+  int32_t update_tile;
+  int32_t ragged_units;
+} socu_tuning;
+
+/* As socu_launch_create, with per-launch settings (NULL: none) applied on top
+ * of the tuned table.  The reference's block_dim maps to the three thread
+ * counts, its block_size to update_tile. */
+int socu_launch_create_tuned(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
+                             const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
+                             int use_cuda_graph, const socu_tuning* settings, void* stream);
+
+/* Install (settings != NULL) or remove the tuned entry for (dtype, n, n_rhs);
+ * n_rhs = 0 is the entry for any n_rhs without one of its own.  Launches
+ * created afterwards (and direct socu_cholesky_* calls, refined and ragged
+ * solves, whose float factor uses the SOCU_FLOAT32 entries) read the table. */
+int socu_tuning_set(socu_dtype dtype, int64_t n, int64_t n_rhs, const socu_tuning* settings);
+
+/* The table's effective entry for (dtype, n, n_rhs) (zeros where unset). */
+int socu_tuning_get(socu_dtype dtype, int64_t n, int64_t n_rhs, socu_tuning* out);
+
+/* Remove every tuned entry. */
+int socu_tuning_clear(void);
+
+/* Kernel kinds of socu_launch_profile. */
+typedef enum socu_kernel_kind {
+  SOCU_KIND_NODE = 0,          /* level node: potrf + coupling solves (+ forward step) */
+  SOCU_KIND_UPDATE = 1,        /* Schur updates and fill-in */
+  SOCU_KIND_PULL = 2,          /* forward coupling updates fused into factor_and_solve */
+  SOCU_KIND_FORWARD = 3,       /* forward sweep */
+  SOCU_KIND_BACKWARD = 4,      /* backward sweep */
+  SOCU_KIND_REFINE_SETUP = 5,  /* refinement: state reset, float copies, norms */
+  SOCU_KIND_REFINE_UPDATE = 6, /* refinement: x += delta */
+  SOCU_KIND_RESIDUAL = 7,      /* refinement: FP64 residual and norms */
+  SOCU_KIND_REFINE_CHECK = 8,  /* refinement: convergence test */
+  SOCU_KIND_RAGGED = 9,        /* ragged batch: queue reset + persistent solver */
+  SOCU_KIND_COUNT = 10
+} socu_kernel_kind;
+
+/* One eager (never graph) run of `launch` on `stream` with a CUDA event pair
+ * around every kernel; synchronises, then ms[k] = summed device time and
+ * launches[k] = kernel count of kind k (arrays of SOCU_KIND_COUNT).  A
+ * refined solve runs all its max_iter rounds.  For measurement only: the
+ * events add gaps between kernels. */
+int socu_launch_profile(socu_launch_t launch, void* stream, double* ms, int64_t* launches);
+
 /* Number of kernels one run enqueues (0 for a NULL launch).  For a
  * graph-captured refined solve: the kernels before the refinement loop. */
 int64_t socu_launch_kernel_count(socu_launch_t launch);
@@ -189,7 +248,11 @@ int socu_refine_fallback_launch_create(socu_launch_t* out, const double* L, cons
  * array's device address up (make that first call before any stream
  * capture).  All calls share the one array: every call re-initialises what it
  * reads, but calls whose work overlaps on the GPU (different streams, or
- * different host threads on the same device) race and corrupt each other. */
+ * different host threads on the same device) race and corrupt each other.
+ * The host cannot see convergence without a synchronisation, so every call
+ * enqueues all max_iter refinement rounds; instances that have converged skip
+ * the work of the remaining rounds (their kernels return at once), which
+ * still costs the launches: pass the smallest max_iter that meets tol. */
 #define SOCU_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 
 int socu_refine_solve_noalloc(const double* L, const double* E, const double* b, double* x, const uint8_t* mask,
@@ -255,7 +318,29 @@ int socu_ragged_error(socu_ragged_t batch, int* flag);
 /* CTAs of the persistent launch (occupancy x SM count). */
 int64_t socu_ragged_grid(socu_ragged_t batch);
 
+/* Bound of one device-side queue wait, in nanoseconds of %globaltimer without
+ * any queue progress (default 4e9, i.e. 4 s; range 1e3 .. 6e10).  A CTA whose
+ * wait runs out sets error word 1 (socu_ragged_error) and returns, so a
+ * stalled queue ends the launch instead of hanging it.  No counterpart in the
+ * reference (its launches do not wait on each other). */
+int socu_ragged_set_wait_limit(socu_ragged_t batch, int64_t timeout_ns);
+
+/* Failure injection for tests of the bound above, host side only: leave the
+ * first-phase tasks of `instance` out of the queue's initial contents, so that
+ * this instance never starts and the queue stalls once the others are done.
+ * The next solve then ends with error word 1.  No counterpart in the reference. */
+int socu_ragged_withhold_instance(socu_ragged_t batch, int64_t instance);
+
 int socu_ragged_destroy(socu_ragged_t batch);
+
+/* Throughput probe of the FP64 tensor-core pipe (mma.sync m8n8k4 .f64 on
+ * register operands, no memory traffic): `blocks` CTAs of `threads` threads,
+ * `iters` steps of 8 independent chains per warp.  *flops receives the
+ * launch's floating-point operations; time the launch with CUDA events on
+ * `stream` to get the device's FP64 tensor peak (the roofline denominator of
+ * the FP64 factor).  `sink` is a device double the kernel may write.  No
+ * counterpart in the reference. */
+int socu_dmma_peak_launch(int64_t blocks, int threads, int iters, double* sink, void* stream, double* flops);
 
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */

@@ -54,6 +54,38 @@ def readme_problem(N: int, n: int, m: int = 1, shift: float = 10.0, seed: int = 
     return L, E, b
 
 
+def illcond_problem(N: int, n: int, m: int = 2, kappa: float = 1e6, alpha: float = 0.3, seed: int = 0):
+    """SPD block-tridiagonal system whose diagonal factor blocks have condition
+    number ~kappa at every separator level; returns (L (N,n,n), E (S,n,n), b (N,n,m)).
+
+    Psi = A^{1/2} M A^{1/2} with A = blockdiag(A_i), A_i = U_i diag(sigma^2) U_i^T
+    (U_i random orthogonal, sigma from 1 down to 1/kappa) and M the block
+    tridiagonal matrix with identity diagonal blocks and alpha * Q_i (Q_i random
+    orthogonal) off the diagonal.  M is well conditioned for alpha < 1/2
+    (eigenvalues in [1 - 2 alpha, 1 + 2 alpha]), so every Schur complement of Psi
+    is A^{1/2}-congruent to one of M: each diagonal factor block C_i is
+    A_i^{1/2} times a well-conditioned matrix and kappa(C_i) ~ kappa, while
+    kappa(Psi) ~ kappa^2 (still positive definite in FP64 up to kappa ~ 1e8).
+    The blocks are genuinely ill conditioned, not merely badly scaled (a
+    diagonal scaling would leave every Cholesky-based method's relative
+    errors unchanged).
+    """
+    rng = np.random.default_rng(seed)
+    sig = np.geomspace(1.0, 1.0 / kappa, n)
+    roots = []
+    for _ in range(N):
+        U, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        roots.append((U * sig) @ U.T)
+    L = np.stack([r @ r for r in roots])
+    L = 0.5 * (L + np.swapaxes(L, -1, -2))
+    E = np.zeros((off_diag_storage_len(N), n, n))
+    for i in range(N - 1):
+        Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        E[i] = alpha * roots[i + 1] @ Q @ roots[i]
+    b = rng.standard_normal((N, n, m))
+    return L, E, b
+
+
 def ragged_instance(seed: int, instance: int):
     """One instance of the ragged MPC-style batch: N ~ U{8..256}, n in {8,16,32,48},
     m in {1,4}, README generator with shift 10, seeded by seed + instance id."""

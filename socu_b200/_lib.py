@@ -36,6 +36,28 @@ OP_FORWARD_INV = 6
 OP_BACKWARD_INV = 7
 OP_SOLVE_INV = 8
 
+KIND_NAMES = ("node", "update", "pull", "forward", "backward", "refine_setup", "refine_update", "residual",
+              "refine_check", "ragged")
+KIND_COUNT = len(KIND_NAMES)
+
+
+class Tuning(ctypes.Structure):
+    """socu_tuning: launch settings, 0 = not set (include/socu_b200.h)."""
+    _fields_ = [("node_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
+                ("sweep_threads", ctypes.c_int32), ("sweep_tensor_cores", ctypes.c_int32),
+                ("update_tile", ctypes.c_int32), ("ragged_units", ctypes.c_int32)]
+
+    FIELDS = ("node_threads", "update_threads", "sweep_threads", "sweep_tensor_cores", "update_tile",
+              "ragged_units")
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(**{k: int(d.get(k, 0) or 0) for k in cls.FIELDS})
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k in self.FIELDS}
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -60,6 +82,12 @@ _SIGNATURES = {
     "socu_launch_create": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p,
                                   _i64, _i64, _i64, _i64, _int, _vp]),
     "socu_launch_run": (_int, [_vp, _vp]),
+    "socu_launch_create_tuned": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p,
+                                        _i64, _i64, _i64, _i64, _int, _vp, _vp]),
+    "socu_tuning_set": (_int, [_int, _i64, _i64, _vp]),
+    "socu_tuning_get": (_int, [_int, _i64, _i64, _vp]),
+    "socu_tuning_clear": (_int, []),
+    "socu_launch_profile": (_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i64)]),
     "socu_launch_kernel_count": (_i64, [_vp]),
     "socu_launch_round_kernel_count": (_i64, [_vp]),
     "socu_launch_destroy": (_int, [_vp]),
@@ -84,6 +112,9 @@ _SIGNATURES = {
                                          _int, _vp]),
     "socu_ragged_error": (_int, [_vp, ctypes.POINTER(_int)]),
     "socu_ragged_grid": (_i64, [_vp]),
+    "socu_ragged_set_wait_limit": (_int, [_vp, _i64]),
+    "socu_ragged_withhold_instance": (_int, [_vp, _i64]),
+    "socu_dmma_peak_launch": (_int, [_i64, _int, _int, _vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "socu_ragged_destroy": (_int, [_vp]),
 }
 

@@ -68,8 +68,11 @@ def _torch_dtype(dtype):
 def optimal_problem_settings(n: int, dtype):
     """Same keys and values as the reference (socu/block_tridiag_solver.py:26-60).
 
-    ``block_dim`` / ``block_size`` do not steer the B200 kernels (their tiling
-    is fixed per n); ``pad_multiple`` drives the JAX frontend's padding.
+    These are the reference's defaults, reported for compatibility; the B200
+    kernels take their launch settings from built-in heuristics or the tuned
+    table (socu_b200.autotune) unless ``block_dim`` / ``block_size`` are
+    passed to a factory explicitly.  ``pad_multiple`` drives the JAX
+    frontend's padding.
     """
     name = _dtype_name(dtype)
     if name == "float64":
@@ -164,7 +167,27 @@ def _validate(L, E, x, mask, with_x: bool):
     return L, E, x, batch_dim, horizon, n, n_rhs
 
 
-def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x):
+def _settings(block_dim, block_size):
+    """Per-launch settings from the reference's tiling arguments: block_dim
+    (threads per tile block) sets the threads per CTA of the node, update and
+    sweep kernels, rounded up to 64, 128 or 256; block_size (tile size of the
+    blocked kernels) sets the output tile of the blocked Schur update, used for
+    n > 64 (16 if block_size <= 16, else 32).  None leaves a setting to the
+    tuned table / heuristics."""
+    out = {}
+    if block_dim is not None:
+        bd = int(block_dim)
+        assert bd > 0, "block_dim must be positive"
+        out["node_threads"] = out["update_threads"] = out["sweep_threads"] = 64 if bd <= 64 else (
+            128 if bd <= 128 else 256)
+    if block_size is not None:
+        bs = int(block_size)
+        assert bs > 0, "block_size must be positive"
+        out["update_tile"] = 16 if bs <= 16 else 32
+    return out or None
+
+
+def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, settings=None):
     L, E = _as_tensor(L), _as_tensor(E)
     x = _as_tensor(x) if with_x else None
     mask = _as_tensor(mask) if mask is not None else None
@@ -188,17 +211,21 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x):
         assert mask.device == dev and mask.is_contiguous(), "mask must be a contiguous array on the solver's device"
 
     lib = _lib.load()
+    from . import autotune
+    autotune.maybe_autotune(tdt, n, n_rhs, dev)
     dt = _lib.FLOAT64 if tdt == torch.float64 else _lib.FLOAT32
     sh = _stream_handle(stream, dev)
     handle = ctypes.c_void_p()
+    tuning = _lib.Tuning.from_dict(settings) if settings else None
     with torch.cuda.device(dev):
         cap_stream = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
-        status = lib.socu_launch_create(
+        status = lib.socu_launch_create_tuned(
             ctypes.byref(handle), op, dt,
             L.data_ptr(), E.data_ptr() if E.numel() else None,
             x.data_ptr() if with_x else None,
             mask.data_ptr() if mask is not None else None,
-            batch, horizon, n, n_rhs, int(bool(use_cuda_graph)), cap_stream)
+            batch, horizon, n, n_rhs, int(bool(use_cuda_graph)),
+            ctypes.byref(tuning) if tuning is not None else None, cap_stream)
     _lib.check(status, "socu_launch_create")
     keep = (L, E, x, mask)
     h = handle.value
@@ -207,11 +234,34 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x):
         s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
         _lib.check(lib.socu_launch_run(h, s), "socu_launch_run")
 
+    def profile():
+        """Device time per kernel kind of one eager run (CUDA events around
+        every kernel; synchronises): {kind: (ms, launches)}."""
+        ms = (ctypes.c_double * _lib.KIND_COUNT)()
+        cnt = (ctypes.c_int64 * _lib.KIND_COUNT)()
+        s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.socu_launch_profile(h, s, ms, cnt), "socu_launch_profile")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES) if cnt[i]}
+
     callback._socu_arrays = keep
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     callback.uses_cuda_graph = bool(use_cuda_graph)
+    callback.profile = profile
+    callback.settings = dict(settings or {})
     weakref.finalize(callback, lib.socu_launch_destroy, h)
     return callback
+
+
+_OPS = {"factor": _lib.OP_FACTOR, "factor_and_solve": _lib.OP_FACTOR_AND_SOLVE, "solve": _lib.OP_SOLVE,
+        "forward": _lib.OP_FORWARD, "backward": _lib.OP_BACKWARD}
+
+
+def _launch_with_settings(op, L, E, x, dtype, settings, use_cuda_graph=True):
+    """Graph-captured launch of `op` (a name of _OPS) with explicit launch
+    settings (the autotuner's candidates)."""
+    with_x = op != "factor"
+    return _create(_OPS[op], L, E, x if with_x else None, None, dtype, None, None, use_cuda_graph, with_x,
+                   settings={k: v for k, v in settings.items() if v})
 
 
 # ---------------------------------------------------------------------------
@@ -226,14 +276,16 @@ def create_cholesky_factor_launch(L, E, mask=None, block_dim=None, block_size=No
     keep_inverse (extension, n <= 64): also store W_i^T = C_i^{-T} in the strict
     upper triangle of every L_i, for the ``factor_has_inverse`` sweeps."""
     op = _lib.OP_FACTOR_INV if keep_inverse else _lib.OP_FACTOR
-    return _create(op, L, E, None, mask, dtype, device, stream, use_cuda_graph, False)
+    return _create(op, L, E, None, mask, dtype, device, stream, use_cuda_graph, False,
+                   _settings(block_dim, block_size))
 
 
 def create_cholesky_factor_and_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
                                             dtype=torch.float64, device=None, stream=None,
                                             use_cuda_graph=False):
     """Factor fused with the forward sweep, then the backward sweep; x: b in, solution out."""
-    return _create(_lib.OP_FACTOR_AND_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+    return _create(_lib.OP_FACTOR_AND_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
+                   _settings(block_dim, block_size))
 
 
 def create_cholesky_forward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
@@ -245,7 +297,8 @@ def create_cholesky_forward_substitution_launch(L, E, x, mask=None, block_dim=No
     upper triangles (factor_and_solve, or factor with keep_inverse=True); the
     sweep then multiplies by W_i instead of solving with C_i."""
     op = _lib.OP_FORWARD_INV if factor_has_inverse else _lib.OP_FORWARD
-    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
+                   _settings(block_dim, block_size))
 
 
 def create_cholesky_backward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,
@@ -257,7 +310,8 @@ def create_cholesky_backward_substitution_launch(L, E, x, mask=None, block_dim=N
     upper triangles (factor_and_solve, or factor with keep_inverse=True); the
     sweep then multiplies by W_i instead of solving with C_i."""
     op = _lib.OP_BACKWARD_INV if factor_has_inverse else _lib.OP_BACKWARD
-    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
+                   _settings(block_dim, block_size))
 
 
 def create_cholesky_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
@@ -269,4 +323,5 @@ def create_cholesky_solve_launch(L, E, x, mask=None, block_dim=None, block_size=
     upper triangles (factor_and_solve, or factor with keep_inverse=True); the
     sweep then multiplies by W_i instead of solving with C_i."""
     op = _lib.OP_SOLVE_INV if factor_has_inverse else _lib.OP_SOLVE
-    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True)
+    return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
+                   _settings(block_dim, block_size))

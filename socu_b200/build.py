@@ -9,12 +9,14 @@ libcudart version a host process (e.g. PyTorch) happens to load.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import hashlib
 import os
 import pathlib
 import shutil
 import subprocess
 import sys
+import tempfile
 
 PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
@@ -23,7 +25,7 @@ OUT_DIR = PKG / "lib"
 OUT = OUT_DIR / "libsocu_b200.so"
 STAMP = OUT_DIR / ".build_stamp"
 
-SOURCES = ["capi.cu"]
+SOURCES = ["capi.cu", "peak.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,24 +45,35 @@ def _digest() -> str:
     return h.hexdigest()
 
 
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd))
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+    return res.returncode
+
+
 def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
     digest = _digest()
     if not force and OUT.exists() and STAMP.exists() and STAMP.read_text() == digest:
         return OUT
     OUT_DIR.mkdir(parents=True, exist_ok=True)
-    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-           "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-           "-I", str(ROOT / "include"),
-           "-o", str(OUT) + ".tmp", *[str(CSRC / s) for s in SOURCES]]
+    nvcc = nvcc_path()
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+             "-I", str(ROOT / "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libsocu_b200.so")
-    if verbose:
-        sys.stderr.write(res.stdout + res.stderr)
+        flags.insert(0, "-Xptxas=-v")
+    with tempfile.TemporaryDirectory(prefix="socu_build_") as tmp:
+        objs = [os.path.join(tmp, pathlib.Path(src).stem + ".o") for src in SOURCES]
+        # translation units compile in parallel, then one link step
+        with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            codes = list(ex.map(lambda so: _run([nvcc, *flags, "-c", "-o", so[1], str(CSRC / so[0])], verbose),
+                                zip(SOURCES, objs)))
+        if any(codes):
+            raise RuntimeError("nvcc failed building libsocu_b200.so")
+        if _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(OUT) + ".tmp", *objs], verbose):
+            raise RuntimeError("nvcc failed linking libsocu_b200.so")
     os.replace(str(OUT) + ".tmp", OUT)
     STAMP.write_text(digest)
     return OUT

@@ -5,8 +5,6 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
-#include <map>
-#include <tuple>
 #include <mutex>
 #include <new>
 #include <utility>
@@ -27,25 +25,34 @@ int cuda_status(cudaError_t e) {
   return SOCU_ERR_CUDA;
 }
 
-std::vector<Level> schedule(int N) {
-  // socu/block_tridiag_solver.py:869-914
-  std::vector<Level> out;
+// Level schedule of a horizon-N system (socu/block_tridiag_solver.py:869-914),
+// written to a caller array of kMaxLevels entries (no heap: the no-allocation
+// entry point shares this path).  Returns the number of levels K.
+constexpr int kMaxLevels = 32;   // horizon <= 2^30
+struct Schedule {
+  Level lv[kMaxLevels];
+  int K = 0;
+  const Level& operator[](int l) const { return lv[l]; }
+};
+
+void schedule(int N, Schedule* out) {
   int s = 1, prev = 0, curr = 0, nxt = N - 1;
   const int K = static_cast<int>(socu_recursive_iterations(N));
+  out->K = K;
   for (int l = 0; l < K; ++l) {
-    Level lv;
+    Level& lv = out->lv[l];
     lv.s = s;
     lv.d = (N + s) / (2 * s);
     lv.oc = curr;
     lv.on = nxt;
     lv.op = prev;
-    out.push_back(lv);
+    lv.tc = 0;
+    lv.tile = kTile;
     s *= 2;
     prev = curr;
     curr = nxt;
     nxt += N / s - 1;
   }
-  return out;
 }
 
 int threads_for(int n) { return n <= 16 ? 64 : (n <= 32 ? 128 : 256); }
@@ -62,23 +69,40 @@ int max_smem_optin() {
   return cached;
 }
 
-// Opt in to large dynamic shared memory once per kernel and size (the
-// attribute is per function and device; a small cache keeps repeated calls
-// off the driver).
+// Small fixed-capacity caches of per-kernel driver queries (static storage,
+// no heap: every solve path, the no-allocation entry point included, uses
+// them).  A full table just stops caching; lookups stay correct.
+constexpr int kCacheSlots = 512;
+
+// Opt in to large dynamic shared memory once per kernel, device and size (the
+// attribute is per function and device).
+struct PrepSlot {
+  const void* fn;
+  int dev;
+  size_t smem;
+};
 std::mutex g_prep_mu;
-std::map<std::pair<const void*, int>, size_t> g_prepared;
+PrepSlot g_prepared[kCacheSlots];
+int g_n_prepared = 0;
 
 template <typename K>
 cudaError_t prepare(K kernel, size_t smem) {
   if (smem <= 48 * 1024) return cudaSuccess;
   int dev = 0;
   cudaGetDevice(&dev);
-  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  const void* fn = reinterpret_cast<const void*>(kernel);
   std::lock_guard<std::mutex> g(g_prep_mu);
-  auto it = g_prepared.find(key);
-  if (it != g_prepared.end() && it->second >= smem) return cudaSuccess;
+  int slot = -1;
+  for (int i = 0; i < g_n_prepared; ++i)
+    if (g_prepared[i].fn == fn && g_prepared[i].dev == dev) {
+      if (g_prepared[i].smem >= smem) return cudaSuccess;
+      slot = i;
+      break;
+    }
   const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess) g_prepared[key] = smem;
+  if (e != cudaSuccess) return e;
+  if (slot < 0 && g_n_prepared < kCacheSlots) slot = g_n_prepared++;
+  if (slot >= 0) g_prepared[slot] = PrepSlot{fn, dev, smem};
   return e;
 }
 
@@ -86,34 +110,127 @@ cudaError_t prepare(K kernel, size_t smem) {
 // CTAs (twice as many resident per SM) finish the level in fewer waves, as on
 // the wide bottom level of the float factor (measured: 80 -> 70 us for 512
 // n = 64 nodes; the Schur-update launches lose more per CTA than the waves
-// save and keep 256).  Occupancies are cached per kernel, device and
-// shared-memory size.
+// save and keep 256).  Occupancies are cached per kernel, device,
+// shared-memory size and thread count.
+struct OccSlot {
+  const void* fn;
+  int dev;
+  size_t smem;
+  int threads, blocks;
+};
 std::mutex g_occ_mu;
-std::map<std::tuple<const void*, int, size_t, int>, int> g_occ;
+OccSlot g_occ[kCacheSlots];
+int g_n_occ = 0;
+
+template <typename K>
+int occupancy(K kernel, int dev, int threads, size_t smem) {
+  const void* fn = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> g(g_occ_mu);
+  for (int i = 0; i < g_n_occ; ++i)
+    if (g_occ[i].fn == fn && g_occ[i].dev == dev && g_occ[i].smem == smem && g_occ[i].threads == threads)
+      return g_occ[i].blocks;
+  int v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess) v = 0;
+  if (g_n_occ < kCacheSlots) g_occ[g_n_occ++] = OccSlot{fn, dev, smem, threads, v};
+  return v;
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  return sms;
+}
 
 template <typename K>
 int level_threads(K kernel, int nth, long long blocks, size_t smem) {
   if (nth != 256 || blocks <= 0) return nth;
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-    return nth;
-  auto occ = [&](int threads) {
-    const auto key = std::make_tuple(reinterpret_cast<const void*>(kernel), dev, smem, threads);
-    std::lock_guard<std::mutex> g(g_occ_mu);
-    auto it = g_occ.find(key);
-    if (it != g_occ.end()) return it->second;
-    int v = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess) v = 0;
-    g_occ[key] = v;
-    return v;
-  };
-  const int o256 = occ(256), o128 = occ(128);
+  int dev = 0;
+  const int sms = sm_count();
+  if (sms <= 0 || cudaGetDevice(&dev) != cudaSuccess) return nth;
+  const int o256 = occupancy(kernel, dev, 256, smem), o128 = occupancy(kernel, dev, 128, smem);
   if (o256 <= 0 || o128 <= 0) return nth;
   const long long w256 = (blocks + (long long)sms * o256 - 1) / ((long long)sms * o256);
   const long long w128 = (blocks + (long long)sms * o128 - 1) / ((long long)sms * o128);
   return w128 < w256 ? 128 : 256;
 }
+
+// ---------------------------------------------------------------------------
+// Launch settings.  Built-in heuristics, replaced field by field by a tuned
+// entry for (dtype, n, n_rhs) -- or for (dtype, n, any n_rhs), stored with
+// n_rhs = 0 -- installed with socu_tuning_set (the autotuner's cache), and by
+// a per-launch override (the reference's block_dim / block_size arguments).
+// A field of 0 means "not set".
+// ---------------------------------------------------------------------------
+struct TuneSlot {
+  int dtype, n, m;
+  socu_tuning t;
+};
+std::mutex g_tune_mu;
+TuneSlot g_tune[kCacheSlots];
+int g_n_tune = 0;
+
+bool tuning_valid(const socu_tuning& t) {
+  auto thr = [](int v) { return v == 0 || v == 64 || v == 128 || v == 256; };
+  return thr(t.node_threads) && thr(t.update_threads) && thr(t.sweep_threads) && t.sweep_tensor_cores >= 0 &&
+         t.sweep_tensor_cores <= 2 && (t.update_tile == 0 || t.update_tile == 16 || t.update_tile == 32) &&
+         t.ragged_units >= 0 && t.ragged_units <= 64;
+}
+
+void tuning_merge(socu_tuning* into, const socu_tuning& over) {
+  if (over.node_threads) into->node_threads = over.node_threads;
+  if (over.update_threads) into->update_threads = over.update_threads;
+  if (over.sweep_threads) into->sweep_threads = over.sweep_threads;
+  if (over.sweep_tensor_cores) into->sweep_tensor_cores = over.sweep_tensor_cores;
+  if (over.update_tile) into->update_tile = over.update_tile;
+  if (over.ragged_units) into->ragged_units = over.ragged_units;
+}
+
+// Tuned entry for (dtype, n, m), falling back to (dtype, n, any m); zeros if none.
+socu_tuning tuning_lookup(int dtype, int n, int m) {
+  socu_tuning out{};
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  int wild = -1, exact = -1;
+  for (int i = 0; i < g_n_tune; ++i) {
+    if (g_tune[i].dtype != dtype || g_tune[i].n != n) continue;
+    if (g_tune[i].m == m) exact = i;
+    else if (g_tune[i].m == 0) wild = i;
+  }
+  if (wild >= 0) tuning_merge(&out, g_tune[wild].t);
+  if (exact >= 0) tuning_merge(&out, g_tune[exact].t);
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// Profiling runs (socu_launch_profile): an event pair around every kernel
+// launch of an eager run, summed per kernel kind afterwards.
+// ---------------------------------------------------------------------------
+struct Prof {
+  std::vector<cudaEvent_t> start, stop;
+  std::vector<int> kind;
+  cudaError_t err = cudaSuccess;
+};
+thread_local Prof* g_prof = nullptr;
+
+void prof_mark(cudaStream_t s, bool begin, int kind) {
+  if (g_prof == nullptr) return;
+  cudaEvent_t e = nullptr;
+  cudaError_t r = cudaEventCreate(&e);
+  if (r == cudaSuccess) r = cudaEventRecord(e, s);
+  if (r != cudaSuccess) {
+    if (g_prof->err == cudaSuccess) g_prof->err = r;
+    if (e) cudaEventDestroy(e);
+    return;
+  }
+  if (begin) {
+    g_prof->start.push_back(e);
+    g_prof->kind.push_back(kind);
+  } else {
+    g_prof->stop.push_back(e);
+  }
+}
+inline void prof_begin(cudaStream_t s, int kind) { prof_mark(s, true, kind); }
+inline void prof_end(cudaStream_t s) { prof_mark(s, false, 0); }
 
 // The library links the CUDA runtime statically, so its notion of the
 // current device is separate from the caller's: follow the device that owns
@@ -188,19 +305,24 @@ struct Fork {
 // inv: the factor carries (FACTOR, FACTOR_AND_SOLVE) or has (SOLVE) its
 // diagonal inverses; only for internal factors or within factor_and_solve.
 // fork (graph capture only): run the forward pulls on a parallel branch.
+// over: per-launch settings (block_dim / block_size), on top of the tuned table.
 template <typename T>
 int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, bool inv = false,
-            const Fork* fork = nullptr) {
-  const std::vector<Level> lv = schedule(p.N);
-  const int K = static_cast<int>(lv.size());
+            const Fork* fork = nullptr, const socu_tuning* over = nullptr) {
   const int n = p.n, nth = threads_for(n);
+  socu_tuning cfg = tuning_lookup(sizeof(T) == 8 ? SOCU_FLOAT64 : SOCU_FLOAT32, n, p.m);
+  if (over) tuning_merge(&cfg, *over);
+  const int tile = cfg.update_tile ? cfg.update_tile : kTile;
+  Schedule lv;
+  schedule(p.N, &lv);
+  const int K = lv.K;
+  for (int l = 0; l < K; ++l) lv.lv[l].tile = tile;
   const bool withY = op == SOCU_OP_FACTOR_AND_SOLVE;
   const size_t sd = smem_node_launch_elems(n, withY ? p.m : 0, sizeof(T)) * sizeof(T);
-  const size_t su = smem_update_launch_elems(n, sizeof(T)) * sizeof(T);
+  const size_t su = smem_update_launch_elems(n, sizeof(T), tile) * sizeof(T);
   const int mm = p.m > 0 ? p.m : 1;
   const bool res = (long long)smem_sweep_res_elems(n, mm) * (long long)sizeof(T) <= (long long)max_smem_optin();
   const size_t ss = (res ? smem_sweep_res_elems(n, mm) : smem_sweep_elems(n, mm)) * sizeof(T);
-  (void)0;
   inv = inv && res && n <= 64;
   auto node_kernel = withY ? (inv ? k_node<T, true, true> : k_node<T, true, false>)
                            : (inv ? k_node<T, false, true> : k_node<T, false, false>);
@@ -209,6 +331,9 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   auto bwd_kernel = res ? (inv ? k_bwd<T, true, true> : k_bwd<T, true>) : k_bwd<T, false>;
   long long launches = 0;
   const bool run = count == nullptr;
+  const int sms = run ? sm_count() : 0;
+  const int upd_thr = cfg.update_threads ? cfg.update_threads : nth;
+  const int swp_thr = cfg.sweep_threads ? cfg.sweep_threads : nth;
 
   if (run) {
     cudaError_t e = cudaSuccess;
@@ -222,16 +347,27 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     if (e != cudaSuccess) return cuda_status(e);
   }
 
-  auto go_on = [&](cudaStream_t s, auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
+  // sweep products on inverse-carrying float factors: tensor cores when the
+  // launch is wider than the resident sweep CTAs (3 per SM), or as tuned
+  auto sweep_level = [&](const Level& L, long long blocks) {
+    Level o = L;
+    if (cfg.sweep_tensor_cores == 1) o.tc = 1;
+    else if (cfg.sweep_tensor_cores == 2) o.tc = 0;
+    else o.tc = sms > 0 && blocks > 3LL * sms;
+    return o;
+  };
+  auto go_on = [&](cudaStream_t s, auto kernel, int kind, long long blocks, size_t smem, const Level& L,
+                   int threads) {
     if (blocks <= 0) return;
     ++launches;
-    if (run) kernel<<<(unsigned)blocks, threads > 0 ? threads : nth, smem, s>>>(p, L);
+    if (!run) return;
+    prof_begin(s, kind);
+    kernel<<<(unsigned)blocks, threads, smem, s>>>(p, L);
+    prof_end(s);
   };
-  auto wide = [&](auto kernel, long long blocks, size_t smem) {
-    return run ? level_threads(kernel, nth, blocks, smem) : nth;
-  };
-  auto go = [&](auto kernel, long long blocks, size_t smem, const Level& L, int threads = 0) {
-    go_on(st, kernel, blocks, smem, L, threads);
+  auto node_threads = [&](long long blocks) {
+    if (cfg.node_threads) return cfg.node_threads;
+    return run ? level_threads(node_kernel, nth, blocks, sd) : nth;
   };
   const bool forked = run && fork != nullptr && fork->ok();
 
@@ -240,32 +376,36 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
       const long long node_blocks = (long long)p.B * L.d;
-      go(node_kernel, node_blocks, sd, L, wide(node_kernel, node_blocks, sd));
+      go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
       if (l + 1 < K) {
         // fused forward: apply this level's updates to every target vector
         const long long pull_blocks = withY ? (long long)p.B * (p.N / lv[l + 1].s) : 0;
+        const Level PL = sweep_level(lv[l + 1], pull_blocks);
         if (forked && pull_blocks > 0) {
           cudaEventRecord(fork->split, st);
           cudaStreamWaitEvent(fork->aux, fork->split, 0);
-          go_on(fork->aux, pull_kernel, pull_blocks, ss, lv[l + 1]);
+          go_on(fork->aux, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
           cudaEventRecord(fork->join, fork->aux);
         }
-        go(k_update<T>, (long long)p.B * update_launch_tasks(n, p.N, L), su, L);
+        go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L, upd_thr);
         if (forked && pull_blocks > 0)
           cudaStreamWaitEvent(st, fork->join, 0);
         else
-          go(pull_kernel, pull_blocks, ss, lv[l + 1]);
+          go_on(st, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
       }
     }
   }
   if (op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE) {
     for (int l = 0; l < K; ++l) {
-      const Level& L = lv[l];
-      go(fwd_kernel, (long long)p.B * (l == 0 ? L.d : p.N / L.s), ss, L);
+      const long long blocks = (long long)p.B * (l == 0 ? lv[l].d : p.N / lv[l].s);
+      go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks), swp_thr);
     }
   }
   if (op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE) {
-    for (int l = K - 1; l >= 0; --l) go(bwd_kernel, (long long)p.B * lv[l].d, ss, lv[l]);
+    for (int l = K - 1; l >= 0; --l) {
+      const long long blocks = (long long)p.B * lv[l].d;
+      go_on(st, bwd_kernel, SOCU_KIND_BACKWARD, blocks, ss, sweep_level(lv[l], blocks), swp_thr);
+    }
   }
   if (count) *count = launches;
   if (run) return cuda_status(cudaGetLastError());
@@ -312,8 +452,8 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
   d->n = (int)n;
   d->m = needs_x ? (int)n_rhs : 0;
   d->S = (int)S;
-  // grid sizes of the widest launches must fit
-  const int nt = ceil_div(d->n, kTile);
+  // grid sizes of the widest launches must fit (smallest update tile: 16)
+  const int nt = ceil_div(d->n, 16);
   const long long per_node = 2LL * nt * nt + 1;
   const long long widest = (long long)d->B * ((d->N + 1) / 2) * per_node + 1;
   if (!grid_ok(widest)) return SOCU_ERR_UNSUPPORTED;
@@ -322,7 +462,7 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
 
 int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask,
              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, cudaStream_t st,
-             long long* count, const Fork* fork = nullptr) {
+             long long* count, const Fork* fork = nullptr, const socu_tuning* over = nullptr) {
   Dims d;
   const int v = validate(op, dtype, L, E, x, batch, horizon, n, n_rhs, &d);
   if (v != SOCU_OK) return v;
@@ -341,8 +481,8 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
   op = base_op(op, &inv);
   inv = inv || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (dtype == SOCU_FLOAT64)
-    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv, fork);
-  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv, fork);
+    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv, fork, over);
+  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv, fork, over);
 }
 
 
@@ -426,14 +566,20 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     const long long nvec = (long long)a.B * a.N * a.n * a.m;
     const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
     const int nrc = ceil_div(a.n, kResRows);
+    prof_begin(st, SOCU_KIND_REFINE_UPDATE);
     k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+    prof_end(st);
+    prof_begin(st, SOCU_KIND_RESIDUAL);
     if (residual_uses_rows(a.n))
       k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
                               smem_residual_x_elems(a.n) * sizeof(double), st>>>(a);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
                          st>>>(a);
+    prof_end(st);
+    prof_begin(st, SOCU_KIND_REFINE_CHECK);
     k_ref_check<<<(a.B + 255) / 256, 256, 0, st>>>(a);
+    prof_end(st);
   } else {
     *count = 3;
   }
@@ -453,12 +599,16 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
     const size_t sinit = smem_ref_init_elems(a.n) * sizeof(double);
     cudaError_t e = prepare(k_residual<true>, sres);
     if (e != cudaSuccess) return cuda_status(e);
+    prof_begin(st, SOCU_KIND_REFINE_SETUP);
     k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
+    prof_end(st);
     const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
+    prof_begin(st, SOCU_KIND_REFINE_SETUP);
     if (residual_uses_rows(a.n))
       k_ref_init_rows<<<init_blocks, 256, sinit, st>>>(a);
     else
       k_ref_init<<<init_blocks, 256, 0, st>>>(a);
+    prof_end(st);
     e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);   // the first test decides
     if (e != cudaSuccess) return cuda_status(e);
   }
@@ -648,6 +798,8 @@ struct socu_ragged_s {
   int* d_rem = nullptr;
   int* d_err = nullptr;
   unsigned int n_init = 0, capacity = 0;
+  std::vector<unsigned long long> init;   // host copy of the queue's initial contents
+  long long timeout_ns = 0;
   float* d_w32 = nullptr;         // refinement: L32 | E32 | R32
   size_t w_off[3] = {0, 0, 0};
   RefineState* d_state = nullptr;
@@ -672,6 +824,7 @@ struct socu_launch_s {
   double tol = 0.0;
   double* eta = nullptr;
   int32_t* iters = nullptr;
+  socu_tuning over{};               // per-launch settings (block_dim / block_size)
 };
 
 namespace {
@@ -686,7 +839,7 @@ int rg_upc(int n) { return n <= 8 ? 8 : (n <= 16 ? 4 : (n <= 32 ? 2 : 1)); }
 
 // Per-instance descriptors and packed offsets, in instance order.
 int rg_layout(const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count,
-              std::vector<RgInst>* out, long long tot[3]) {
+              std::vector<RgInst>* out, long long tot[3], int dtype = SOCU_FLOAT64) {
   if (count < 0) return SOCU_ERR_INVALID_ARGUMENT;
   if (count >= (1LL << kRgInstBits)) return SOCU_ERR_UNSUPPORTED;
   if (count > 0 && (horizon == nullptr || n == nullptr || n_rhs == nullptr)) return SOCU_ERR_INVALID_ARGUMENT;
@@ -701,7 +854,8 @@ int rg_layout(const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, in
     I.m = (int)n_rhs[i];
     I.S = (int)socu_off_diag_storage_len(horizon[i]);
     I.K = (int)socu_recursive_iterations(horizon[i]);
-    I.upc = rg_upc(I.n);
+    const int tu = tuning_lookup(dtype, I.n, I.m).ragged_units;
+    I.upc = tu > 0 ? tu : rg_upc(I.n);
     I.oL = oL;
     I.oE = oE;
     I.oX = oX;
@@ -741,7 +895,7 @@ int rg_prepare_kernel(socu_ragged_s* r) {
 }
 
 int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const int64_t* n_rhs, int64_t count) {
-  int st = rg_layout(horizon, n, n_rhs, count, &r->inst, r->tot);
+  int st = rg_layout(horizon, n, n_rhs, count, &r->inst, r->tot, r->refine ? SOCU_FLOAT32 : r->dtype);
   if (st != SOCU_OK) return st;
   r->count = (int)count;
   if (count == 0) return SOCU_OK;
@@ -765,7 +919,8 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
     const RgInst &A = r->inst[a], &B = r->inst[b];
     return (double)A.N * A.n * A.n * A.n > (double)B.N * B.n * B.n * B.n;
   });
-  std::vector<unsigned long long> init;
+  std::vector<unsigned long long>& init = r->init;
+  init.clear();
   for (int i : order) {
     const int c = rg_chunks(rg_phase(r->inst[i], mode, 0));
     for (int j = 0; j < c; ++j) init.push_back(rg_encode(i, 0, j));
@@ -826,14 +981,16 @@ int rg_launch(socu_ragged_s* r, RgArgs<T> a, cudaStream_t st) {
   a.q.n_init = r->n_init;
   a.q.capacity = r->capacity;
   a.vc = r->vc;
-  a.timeout_ns = kRgTimeoutNs;
+  a.timeout_ns = r->timeout_ns > 0 ? r->timeout_ns : kRgTimeoutNs;
   cudaError_t e = cudaMemsetAsync(r->d_slot + r->n_init, 0,
                                   sizeof(unsigned long long) * (r->capacity - r->n_init), st);
   if (e != cudaSuccess) return cuda_status(e);
   const long long work = std::max<long long>(r->n_init, r->count);
   const int sb = (int)std::min<long long>((work + 255) / 256, 1024);
+  prof_begin(st, SOCU_KIND_RAGGED);
   k_rg_start<T, MODE><<<sb, 256, 0, st>>>(a);
   k_ragged<T, MODE><<<r->grid, kRgThreads, r->smem, st>>>(a);
+  prof_end(st);
   return cuda_status(cudaGetLastError());
 }
 
@@ -905,7 +1062,7 @@ int launch_enqueue(socu_launch_s* h, cudaStream_t st, const Fork* fork = nullptr
     return refine_enqueue(h->ra, st, nullptr);
   }
   return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st, nullptr,
-                  fork);
+                  fork, &h->over);
 }
 
 // Capture one run into a CUDA graph on a private stream (the legacy default
@@ -958,7 +1115,7 @@ int capture(socu_launch_s* h) {
 // is being captured into a CUDA graph.  For them the float factor, the
 // correction vector and the per-instance refinement state live in the fixed
 // array below instead of a caller workspace.  The host side uses only stack
-// storage.
+// and static storage.
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // == SOCU_NOALLOC_SCRATCH_BYTES
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -987,86 +1144,6 @@ int noalloc_scratch(void** out) {
   return SOCU_OK;
 }
 
-template <typename K>
-cudaError_t noalloc_smem(K kernel, size_t smem) {
-  return smem > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                          : cudaSuccess;
-}
-
-// Same kernel sequence as refine_enqueue, with the level schedule on the stack.
-int refine_enqueue_noalloc(const RefineArgs& a, cudaStream_t st) {
-  Level lv[32];
-  int K = 0;
-  for (int s = 1, prev = 0, curr = 0, nxt = a.N - 1; K < (int)socu_recursive_iterations(a.N); ++K) {
-    lv[K].s = s;
-    lv[K].d = (a.N + s) / (2 * s);
-    lv[K].oc = curr;
-    lv[K].on = nxt;
-    lv[K].op = prev;
-    s *= 2;
-    prev = curr;
-    curr = nxt;
-    nxt += a.N / s - 1;
-  }
-  const Dims d{a.B, a.N, a.n, a.m, a.S};
-  const Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
-  const int n = a.n, nth = threads_for(n);
-  const size_t sd = smem_node_launch_elems(n, a.m, sizeof(float)) * sizeof(float);
-  const size_t su = smem_update_launch_elems(n, sizeof(float)) * sizeof(float);
-  const bool res = (long long)smem_sweep_res_elems(n, a.m) * (long long)sizeof(float) <= (long long)max_smem_optin();
-  const size_t ss = (res ? smem_sweep_res_elems(n, a.m) : smem_sweep_elems(n, a.m)) * sizeof(float);
-  const size_t sres = smem_residual_elems(n) * sizeof(double);
-  const bool inv = use_inverse<float>(n, a.m);
-  auto node = inv ? k_node<float, true, true> : k_node<float, true, false>;
-  auto fwd = res ? (inv ? k_fwd<float, true, false, true> : k_fwd<float, true>) : k_fwd<float, false>;
-  auto pull = res ? k_fwd<float, true, true> : k_fwd<float, false, true>;
-  auto bwd = res ? (inv ? k_bwd<float, true, true> : k_bwd<float, true>) : k_bwd<float, false>;
-  cudaError_t e = noalloc_smem(node, sd);
-  if (e == cudaSuccess) e = noalloc_smem(k_update<float>, su);
-  if (e == cudaSuccess) e = noalloc_smem(fwd, ss);
-  if (e == cudaSuccess) e = noalloc_smem(pull, ss);
-  if (e == cudaSuccess) e = noalloc_smem(bwd, ss);
-  if (e == cudaSuccess) e = noalloc_smem(k_residual<true>, sres);
-  const size_t sinit = smem_ref_init_elems(n) * sizeof(double);
-  if (e != cudaSuccess) return cuda_status(e);
-  (void)0;
-  const int nrc = ceil_div(n, kResRows);
-  const long long nvec = (long long)a.B * a.N * a.n * a.m;
-  const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
-  const int chk_blocks = (a.B + 255) / 256;
-  e = cudaMemsetAsync(a.any_active, 0, sizeof(int), st);
-  if (e != cudaSuccess) return cuda_status(e);
-  k_ref_reset<<<chk_blocks, 256, 0, st>>>(a);
-  const bool rows = residual_uses_rows(n);
-  const unsigned init_blocks = (unsigned)((long long)a.B * (a.N > a.S ? a.N : a.S));
-  if (rows)
-    k_ref_init_rows<<<init_blocks, 256, sinit, st>>>(a);
-  else
-    k_ref_init<<<init_blocks, 256, 0, st>>>(a);
-  // first round fused into the float factor: factor_and_solve of R32 = b
-  for (int l = 0; l < K; ++l) {
-    node<<<(unsigned)((long long)a.B * lv[l].d), nth, sd, st>>>(pf, lv[l]);
-    if (l + 1 < K) {
-      const long long blocks = (long long)a.B * update_launch_tasks(n, a.N, lv[l]);
-      if (blocks > 0) k_update<float><<<(unsigned)blocks, nth, su, st>>>(pf, lv[l]);
-      pull<<<(unsigned)((long long)a.B * (a.N / lv[l + 1].s)), nth, ss, st>>>(pf, lv[l + 1]);
-    }
-  }
-  for (int it = 0; it < a.max_iter; ++it) {
-    if (it > 0)
-      for (int l = 0; l < K; ++l)
-        fwd<<<(unsigned)((long long)a.B * (l == 0 ? lv[l].d : a.N / lv[l].s)), nth, ss, st>>>(pf, lv[l]);
-    for (int l = K - 1; l >= 0; --l) bwd<<<(unsigned)((long long)a.B * lv[l].d), nth, ss, st>>>(pf, lv[l]);
-    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
-    if (rows)
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
-                              smem_residual_x_elems(a.n) * sizeof(double), st>>>(a);
-    else
-      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, sres, st>>>(a);
-    k_ref_check<<<chk_blocks, 256, 0, st>>>(a);
-  }
-  return cuda_status(cudaGetLastError());
-}
 }  // namespace
 
 extern "C" {
@@ -1162,10 +1239,18 @@ int socu_cholesky_run(socu_op op, socu_dtype dtype, void* L, void* E, void* x, c
 int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
                        const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                        int use_cuda_graph, void* stream) {
+  return socu_launch_create_tuned(out, op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, use_cuda_graph, nullptr,
+                                  stream);
+}
+
+int socu_launch_create_tuned(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
+                             const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
+                             int use_cuda_graph, const socu_tuning* settings, void* stream) {
   if (out == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
   *out = nullptr;
+  if (settings && !tuning_valid(*settings)) return SOCU_ERR_INVALID_ARGUMENT;
   long long kernels = 0;
-  int st = dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, nullptr, &kernels);
+  int st = dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, nullptr, &kernels, nullptr, settings);
   if (st != SOCU_OK) return st;
   socu_launch_s* h = new (std::nothrow) socu_launch_s();
   if (!h) return SOCU_ERR_UNSUPPORTED;
@@ -1182,6 +1267,7 @@ int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L
   h->kernels = kernels;
   h->graph = nullptr;
   h->exec = nullptr;
+  if (settings) h->over = *settings;
   if (use_cuda_graph && batch > 0) {
     st = capture(h);
     if (st != SOCU_OK) {
@@ -1402,6 +1488,73 @@ int socu_refine_fallback_launch_create(socu_launch_t* out, const double* L, cons
   return SOCU_OK;
 }
 
+int socu_tuning_set(socu_dtype dtype, int64_t n, int64_t n_rhs, const socu_tuning* settings) {
+  if ((dtype != SOCU_FLOAT32 && dtype != SOCU_FLOAT64) || n <= 0 || n > 4096 || n_rhs < 0 || n_rhs > (1 << 20))
+    return SOCU_ERR_INVALID_ARGUMENT;
+  if (settings && !tuning_valid(*settings)) return SOCU_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (int i = 0; i < g_n_tune; ++i) {
+    TuneSlot& t = g_tune[i];
+    if (t.dtype == (int)dtype && t.n == (int)n && t.m == (int)n_rhs) {
+      if (settings) {
+        t.t = *settings;
+      } else {
+        g_tune[i] = g_tune[--g_n_tune];
+      }
+      return SOCU_OK;
+    }
+  }
+  if (!settings) return SOCU_OK;
+  if (g_n_tune >= kCacheSlots) return SOCU_ERR_UNSUPPORTED;
+  g_tune[g_n_tune++] = TuneSlot{(int)dtype, (int)n, (int)n_rhs, *settings};
+  return SOCU_OK;
+}
+
+int socu_tuning_get(socu_dtype dtype, int64_t n, int64_t n_rhs, socu_tuning* out) {
+  if (out == nullptr || (dtype != SOCU_FLOAT32 && dtype != SOCU_FLOAT64) || n <= 0 || n_rhs < 0)
+    return SOCU_ERR_INVALID_ARGUMENT;
+  *out = tuning_lookup(dtype, (int)n, (int)n_rhs);
+  return SOCU_OK;
+}
+
+int socu_tuning_clear(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_n_tune = 0;
+  return SOCU_OK;
+}
+
+int socu_launch_profile(socu_launch_t h, void* stream, double* ms, int64_t* launches) {
+  if (h == nullptr || ms == nullptr || launches == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < SOCU_KIND_COUNT; ++k) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Prof prof;
+  g_prof = &prof;
+  int s = launch_enqueue(h, st);
+  g_prof = nullptr;
+  cudaError_t e = prof.err;
+  if (s == SOCU_OK && e == cudaSuccess && !prof.stop.empty()) e = cudaEventSynchronize(prof.stop.back());
+  if (s == SOCU_OK && e == cudaSuccess && prof.start.size() == prof.stop.size()) {
+    for (size_t i = 0; i < prof.start.size(); ++i) {
+      float t = 0.f;
+      const cudaError_t r = cudaEventElapsedTime(&t, prof.start[i], prof.stop[i]);
+      if (r != cudaSuccess) {
+        e = r;
+        break;
+      }
+      const int k = prof.kind[i] >= 0 && prof.kind[i] < SOCU_KIND_COUNT ? prof.kind[i] : SOCU_KIND_COUNT - 1;
+      ms[k] += t;
+      launches[k] += 1;
+    }
+  }
+  for (cudaEvent_t ev : prof.start) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : prof.stop) cudaEventDestroy(ev);
+  if (s != SOCU_OK) return s;
+  return cuda_status(e);
+}
+
 int socu_launch_destroy(socu_launch_t h) {
   if (h == nullptr) return SOCU_OK;
   if (h->exec) cudaGraphExecDestroy(h->exec);
@@ -1430,7 +1583,9 @@ int socu_refine_solve_noalloc(const double* L, const double* E, const double* b,
   const int st = noalloc_scratch(&scratch);
   if (st != SOCU_OK) return st;
   const RefineArgs a = refine_args(L, E, b, x, mask, d, max_iter, tol, scratch, eta, iters);
-  return refine_enqueue_noalloc(a, static_cast<cudaStream_t>(stream));
+  // the same enqueue path as socu_refine_solve (level schedule on the stack,
+  // kernel attributes from static caches): only the scratch differs
+  return refine_enqueue(a, static_cast<cudaStream_t>(stream), nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -1535,6 +1690,31 @@ int socu_ragged_error(socu_ragged_t r, int* flag) {
 }
 
 int64_t socu_ragged_grid(socu_ragged_t r) { return r ? r->grid : 0; }
+
+int socu_ragged_set_wait_limit(socu_ragged_t r, int64_t timeout_ns) {
+  if (r == nullptr || timeout_ns < 1000 || timeout_ns > 60000000000LL) return SOCU_ERR_INVALID_ARGUMENT;
+  r->timeout_ns = timeout_ns;
+  return SOCU_OK;
+}
+
+int socu_ragged_withhold_instance(socu_ragged_t r, int64_t instance) {
+  if (r == nullptr || instance < 0 || instance >= r->count) return SOCU_ERR_INVALID_ARGUMENT;
+  std::vector<unsigned long long> kept;
+  kept.reserve(r->init.size());
+  for (unsigned long long t : r->init) {
+    int ii, ph, chunk;
+    rg_decode(t, ii, ph, chunk);
+    if (ii != (int)instance) kept.push_back(t);
+  }
+  if (kept.size() == r->init.size()) return SOCU_OK;
+  int s = rg_device(r);
+  if (s != SOCU_OK) return s;
+  r->init.swap(kept);
+  r->n_init = (unsigned)r->init.size();
+  if (r->n_init == 0) return SOCU_OK;
+  return cuda_status(cudaMemcpy(r->d_init, r->init.data(), sizeof(unsigned long long) * r->n_init,
+                                cudaMemcpyHostToDevice));
+}
 
 int socu_ragged_destroy(socu_ragged_t r) {
   if (r == nullptr) return SOCU_OK;

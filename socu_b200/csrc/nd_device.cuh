@@ -57,6 +57,8 @@ struct Level {
   int oc;   // offset of this level's slots
   int on;   // offset of the next level's slots
   int op;   // offset of the previous level's slots (unused at level 0)
+  int tc;   // sweeps on inverse-carrying factors: 1 = FP64 tensor-core (DMMA) products, 0 = SIMT row dots
+  int tile; // output tile of the blocked Schur update (n > 64): 16 or 32
 };
 
 // ---------------------------------------------------------------------------

@@ -42,9 +42,10 @@ __host__ __device__ inline long long smem_node_elems(int n, int es) {
   return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n), es);
 }
 __host__ __device__ inline int update_ld(int k, int es) { return gemm_ld(k, es); }
-__host__ __device__ inline long long smem_update_elems(int n, int es) {
-  const long long a = 2LL * kTile * update_ld(2 * n, es);
-  const long long f = (long long)kTile * update_ld(n, es) + (long long)n * update_ld(kTile, es);
+// blocked Schur update (n > 64) with tile x tile output tiles
+__host__ __device__ inline long long smem_update_elems(int n, int es, int tile = kTile) {
+  const long long a = 2LL * tile * update_ld(2 * n, es);
+  const long long f = (long long)tile * update_ld(n, es) + (long long)n * update_ld(tile, es);
   return a > f ? a : f;
 }
 __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
@@ -239,7 +240,7 @@ __device__ __forceinline__ void lower_tile_index(int lt, int& ta, int& tc) {
 // Number of output tiles of one update level per instance: U targets with
 // nlt lower tiles each, then d-1 fill-in blocks with nt*nt tiles each.
 __host__ __device__ inline int update_tiles(int n, int N, const Level& lv) {
-  const int nt = ceil_div(n, kTile);
+  const int nt = ceil_div(n, lv.tile);
   return (N / (2 * lv.s)) * (nt * (nt + 1) / 2) + (lv.d - 1) * nt * nt;
 }
 
@@ -249,7 +250,8 @@ __device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv
                                             unsigned char* smem_raw) {
   constexpr int es = sizeof(T);
   const int n = p.n, N = p.N, s = lv.s;
-  const int nt = ceil_div(n, kTile);
+  const int tile = lv.tile;
+  const int nt = ceil_div(n, tile);
   const int nlt = nt * (nt + 1) / 2;
   const int U = N / (2 * s);
   T* Ab = reinterpret_cast<T*>(smem_raw);
@@ -262,12 +264,12 @@ __device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv
     const T* F = p.Eb(b, lv.oc + 2 * (u - 1));
     const bool hasG = j + s < N;
     const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
-    const int r0 = ta * kTile, wa = min_i(kTile, n - r0);
-    const int c0 = tc * kTile, wc = min_i(kTile, n - c0);
+    const int r0 = ta * tile, wa = min_i(tile, n - r0);
+    const int c0 = tc * tile, wc = min_i(tile, n - c0);
     const bool diag = ta == tc;
     const int K = hasG ? 2 * n : n;
     const int lda = update_ld(K, es);       // rows of [F | G^T]
-    T* Bb = Ab + kTile * lda;
+    T* Bb = Ab + tile * lda;
     T* Bop = diag ? Ab : Bb;
     // Ab[r][k] = F[r0+r][k], Ab[r][n+k] = G[k][r0+r]   (k < n)
     async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);
@@ -294,10 +296,10 @@ __device__ __forceinline__ void update_body(const Problem<T>& p, const Level& lv
     const T* F = p.Eb(b, lv.oc + 2 * t);
     const T* G = p.Eb(b, lv.oc + 2 * t - 1);
     T* X = p.Eb(b, lv.on + t - 1);
-    const int r0 = ta * kTile, wa = min_i(kTile, n - r0);
-    const int c0 = tc * kTile, wc = min_i(kTile, n - c0);
-    const int lda = update_ld(n, es), ldg = update_ld(kTile, es);
-    T* Bb = Ab + kTile * lda;
+    const int r0 = ta * tile, wa = min_i(tile, n - r0);
+    const int c0 = tc * tile, wc = min_i(tile, n - c0);
+    const int lda = update_ld(n, es), ldg = update_ld(tile, es);
+    T* Bb = Ab + tile * lda;
     async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);   // F rows
     async_load(Bb, ldg, G + c0, n, wc, n);                    // G columns, n x wc
     cp_async_wait_all();
@@ -370,8 +372,8 @@ __host__ __device__ inline bool update_uses_full(int n) { return n <= kNodeGemmM
 __host__ __device__ inline int update_launch_tasks(int n, int N, const Level& lv) {
   return update_uses_full(n) ? update_blocks(N, lv) : update_tiles(n, N, lv);
 }
-__host__ __device__ inline long long smem_update_launch_elems(int n, int es) {
-  return update_uses_full(n) ? smem_update_full_elems(n, es) : smem_update_elems(n, es);
+__host__ __device__ inline long long smem_update_launch_elems(int n, int es, int tile = kTile) {
+  return update_uses_full(n) ? smem_update_full_elems(n, es) : smem_update_elems(n, es, tile);
 }
 
 template <typename T>
@@ -661,18 +663,17 @@ __device__ __forceinline__ void res_matvec(T* Yout, const T* Z, int ldy, int mc,
 // two accumulators per product (alternate k-steps).  Fragment layout: a0 =
 // A[g][t], b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}] (g = lane / 4, t = lane % 4).
 // ---------------------------------------------------------------------------
-// FP64 sweeps always take the tensor-core products (faster at every level);
-// FP32 sweeps only in launches of more than three CTAs per SM (more than one
-// wave of resident sweep CTAs), which are throughput-bound (measured at
-// N=1024, n=64: bottom level 17.0 -> 15.7 us), while the dependent DMMA chain
-// costs ~0.6 us per node on the 1-256-CTA levels and in the persistent ragged
-// CTAs, where the SIMT products are faster.
+// Sweep products on inverse-carrying factors: FP64 sweeps always take the
+// tensor-core products (faster at every level); FP32 sweeps only in launches
+// wider than one wave of resident sweep CTAs, which are throughput-bound
+// (measured at N=1024, n=64: bottom level 17.0 -> 15.7 us), while the
+// dependent DMMA chain costs ~0.6 us per node on the 1-256-CTA levels and in
+// the persistent ragged CTAs, where the SIMT products are faster.  The host
+// decides per launch (Level::tc, from the launch width and the device's SM
+// count, or from a tuned setting).
 template <typename T>
-__device__ __forceinline__ bool sweep_uses_dmma() {
-  if (sizeof(T) == 8) return true;
-  unsigned nsm;
-  asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
-  return gridDim.x > 3 * nsm;
+__device__ __forceinline__ bool sweep_uses_dmma(const Level& lv) {
+  return sizeof(T) == 8 || lv.tc != 0;
 }
 
 template <typename T, int MODE, bool TR>
@@ -853,7 +854,7 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
       if (c0 == 0 && solve)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
       // Y -= F y_{j-h} + G^T y_{j+h}
-      const bool tc = INV && sweep_uses_dmma<T>();
+      const bool tc = INV && sweep_uses_dmma<T>(lv);
       if (pull) {
         if (tc)
           dmma_product<T, 0, false, true>(Y, Z1, Fs, ldm, G ? Z2 : nullptr, G ? Gs : nullptr, ldm, ldy, mc, nullptr, n);
@@ -934,7 +935,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
       if (c0 == 0)
         for (int r = threadIdx.x; r < n; r += blockDim.x) dv[r] = T(1) / Cs[r * ldm + r];
       // Y -= F^T x_{i+s} + G x_{i-s}
-      const bool tc = INV && sweep_uses_dmma<T>();
+      const bool tc = INV && sweep_uses_dmma<T>(lv);
       if (right || left) {
         if (tc)
           dmma_product<T, 0, true, false>(Y, right ? Z1 : nullptr, right ? Fs : nullptr, ldm, left ? Z2 : nullptr,

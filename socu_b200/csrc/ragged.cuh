@@ -82,6 +82,8 @@ __host__ __device__ inline Level rg_level(int N, int l) {
   lv.oc = curr;
   lv.on = nxt;
   lv.op = prev;
+  lv.tc = 0;       // persistent CTAs: SIMT sweep products (lower latency per node)
+  lv.tile = 32;    // unused (n <= 64: whole-block updates)
   return lv;
 }
 

@@ -150,6 +150,19 @@ class RaggedBatch:
         """CTAs of the persistent kernel."""
         return int(_lib.load().socu_ragged_grid(self._handle))
 
+    def set_wait_limit(self, seconds):
+        """Bound of one device-side queue wait without queue progress (default
+        4 s).  A wait that runs out sets error word 1 and ends its CTA, so a
+        stalled queue ends the launch instead of hanging the GPU."""
+        ns = int(round(float(seconds) * 1e9))
+        _lib.check(_lib.load().socu_ragged_set_wait_limit(self._handle, ns), "socu_ragged_set_wait_limit")
+
+    def withhold_instance(self, i):
+        """Failure injection for tests (host side): leave instance i's first
+        tasks out of the queue, so the next solve stalls and must end through
+        the wait limit with error word 1."""
+        _lib.check(_lib.load().socu_ragged_withhold_instance(self._handle, int(i)), "socu_ragged_withhold_instance")
+
 
 def _storage_len(N):
     return int(_lib.load().socu_off_diag_storage_len(N))

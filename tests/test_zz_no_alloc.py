@@ -6,9 +6,14 @@ allocator and the handler must not call cudaMalloc), a real-time control loop
 that bans allocation after start-up, or code running under CUDA stream
 capture.  It keeps its scratch in a fixed array inside the library instead of
 a caller workspace.  These tests compare it with socu_refine_solve (same
-kernels, caller-provided workspace) on two different problems in a row, so
-that left-over contents of the shared array from the first call would show up
-in the second.  This file is collected last on purpose.
+kernels, caller-provided workspace) on problems of different sizes in a
+row, so that left-over contents of the shared array from an earlier call would
+show up in a later one, and checks each result against the CPU oracle: the
+oracle's backward error of x must meet the tolerance, and x must agree with the
+oracle's FP64 solution within cond(Psi) times that tolerance.  The block sizes
+cover the float node kernel's narrow (n <= 32) and wide (n = 64, 256-thread
+CTAs, tensor-core Schur update) launch shapes.  This file is collected last
+on purpose.
 """
 import ctypes
 
@@ -16,7 +21,7 @@ import numpy as np
 import pytest
 import torch
 
-from oracle import generators
+from oracle import generators, nd_cholesky as nd
 from socu_b200 import _lib
 
 pytestmark = pytest.mark.gpu
@@ -62,9 +67,10 @@ def _run_noalloc(lib, L, E, b, B, N, n, m):
 
 def test_noalloc_matches_workspace_entry_point_on_two_calls():
     lib = _lib.load()
-    # the second problem is smaller, so stale contents of the shared scratch
-    # from the first call would be picked up if anything were not re-initialised
-    for (N, n, m, B, seed) in [(37, 24, 3, 3, 1), (20, 16, 1, 2, 2)]:
+    # later problems are smaller than earlier ones, so stale contents of the
+    # shared scratch from an earlier call would be picked up if anything were
+    # not re-initialised
+    for (N, n, m, B, seed) in [(37, 24, 3, 3, 1), (16, 64, 2, 2, 3), (20, 16, 1, 2, 2)]:
         L, E, b = _problem(N, n, m, B, seed)
         assert lib.socu_refine_workspace_bytes(B, N, n, m) <= 16 << 20
         x_ref, eta_ref, it_ref = _run_workspace(lib, L, E, b, B, N, n, m)
@@ -73,6 +79,14 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
         assert torch.equal(it, it_ref)
         scale = float(x_ref.abs().max())
         assert float((x - x_ref).abs().max()) <= 1e-12 * scale
+        # against the CPU oracle, instance by instance
+        Ln, En, bn, xn = (a.cpu().numpy() for a in (L, E, b, x))
+        for k in range(B):
+            assert nd.backward_error(Ln[k], En[k], xn[k], bn[k])[0] <= TOL
+            _, _, x_ora = nd.nd_factor_and_solve(Ln[k], En[k], bn[k])
+            kappa = np.linalg.cond(generators.dense_from_blocks(Ln[k], En[k]))
+            err = np.abs(xn[k] - x_ora[0]).max() / np.abs(x_ora[0]).max()
+            assert err <= 20 * kappa * TOL + 1e-14, (err, kappa)
 
 
 def test_noalloc_rejects_problems_larger_than_its_scratch():
