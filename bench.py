@@ -2,16 +2,20 @@
 versus the plain FP64 path, at normwise relative backward error <= 1e-12.
 
 Workload: N=1024 blocks, n=64, m=8 right-hand sides, diagonal shift s=10,
-one system per GPU (README generator, seeded).  A step is one full solve of
-that system from its original blocks: float factor + refinement for the
-headline value, FP64 factor_and_solve for the comparison line.
+one system per GPU (README construction, seeded torch CPU generator, so both
+arms solve bit-identical inputs).  A step is one full solve of that system
+from its original blocks: float factor + refinement for the headline value,
+FP64 factor_and_solve for the comparison line.  Further sections (same run,
+same JSON line): the large stress shape N=16384, n=128, m=32; a ragged batch
+of 4096 uneven systems; the differentiable solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun every rank solves its own replica (the path does not shard);
-value = systems solved by all ranks / max-over-ranks time.  The reference arm
-times the CPU oracle (NumPy restatement of the reference algorithm) on the
-host cores, rank 0 only.
+Under torchrun every rank solves its own replica of the single system (the
+path does not shard) and its own contiguous share of the ragged batch
+(instances balanced by factor work); value = systems solved by all ranks /
+max-over-ranks time.  The reference arm times the CPU oracle (NumPy
+restatement of the reference algorithm) on the host cores, rank 0 only.
 """
 from __future__ import annotations
 
@@ -45,20 +49,43 @@ RAGGED_COUNT, RAGGED_SEED = 4096, 0
 # profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md
 TRAFFIC_BYTES = 5005218
 TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md"
+# DRAM bytes (read + write) per k_node<float, y, inverse> launch of the mixed
+# solve (ncu capture): none committed yet
+NODE_TRAFFIC_BYTES = None
+NODE_TRAFFIC_NOTE = "no ncu capture of k_node<float> committed"
 RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
                    "instance i seeded with 0 + i, one persistent launch per solve")
 
 
-def make_problem_gpu(dev):
-    """The workload system on the device (README construction, torch generator)."""
-    from socu_b200.problems import readme_blocks
-    return readme_blocks(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED, batch=1, device=dev)
-
-
 def make_problem_host():
-    """The workload system on the host for the reference arm (NumPy generator, same construction)."""
-    from oracle.generators import readme_problem
-    return readme_problem(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED)
+    """The workload system as float64 CPU tensors (B=1): README construction
+    from a seeded torch CPU generator.  Both arms start from these values."""
+    from socu_b200.problems import readme_blocks
+    return readme_blocks(N_BLOCKS, BLOCK, NRHS, shift=SHIFT, seed=SEED, batch=1, device="cpu")
+
+
+def band_solve_fp64(L, E, b):
+    """FP64 solve of one system by LAPACK's banded Cholesky (scipy
+    solveh_banded, half-bandwidth 2n-1): the dense FP64 solution the forward
+    errors are measured against (a dense matrix of N n unknowns does not fit)."""
+    import scipy.linalg as la
+    N, n = L.shape[0], L.shape[1]
+    m = b.shape[-1]
+    bw = 2 * n - 1
+    ab = np.zeros((bw + 1, N * n))
+    r, c = np.tril_indices(n)
+    for i in range(N):
+        # lower(D_i): ab[k, j] = A[j + k, j]
+        ab[r - c, i * n + c] = L[i][r, c]
+        if i < N - 1:
+            rr, cc = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+            ab[(n + rr - cc).ravel(), (i * n + cc).ravel()] = E[i][rr, cc].ravel()
+    return la.solveh_banded(ab, b.reshape(N * n, m), lower=True).reshape(N, n, m)
+
+
+def forward_error(x, x_ref):
+    """max |x - x_ref| / max |x_ref| (normwise, infinity norm)."""
+    return float(np.abs(x - x_ref).max() / max(np.abs(x_ref).max(), 1e-300))
 
 
 def algorithmic_factor_flops(N, n):
@@ -146,20 +173,33 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle port (NumPy restatement of the reference algorithm)
 # ---------------------------------------------------------------------------
-def cpu_oracle_solves_per_s(L, E, b, reps):
+CPU_SAMPLE_S = 10.0
+
+
+def cpu_oracle_solves_per_s(L, E, b, budget_s=CPU_SAMPLE_S, max_reps=40):
+    """Median time of full FP64 factor_and_solve runs of the oracle, repeated
+    for about budget_s seconds of CPU work (at least 3 runs)."""
     from oracle import nd_cholesky as nd
     ts = []
-    for _ in range(reps):
+    t_start = time.perf_counter()
+    while len(ts) < 3 or (time.perf_counter() - t_start < budget_s and len(ts) < max_reps):
         t0 = time.perf_counter()
         nd.nd_factor_and_solve(L, E, b)
         ts.append(time.perf_counter() - t0)
     return 1.0 / statistics.median(ts), ts
 
 
+def workload_config():
+    return {"workload": WORKLOAD, "N": N_BLOCKS, "n": BLOCK, "m": NRHS, "shift": SHIFT, "tol": TOL,
+            "max_iter": MAX_ITER, "l2": "256 MB flush before every timed step (GPU arm); host CPU run (reference)",
+            "inputs": "README construction, torch CPU generator seed 0, identical in both arms"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
-    L, E, b = make_problem_host()
+    L0, E0, b0 = make_problem_host()
+    L, E, b = L0[0].numpy(), E0[0].numpy(), b0[0].numpy()
     cores = len(os.sched_getaffinity(0))
     from oracle import nd_cholesky as nd
     for _ in range(args.warmup):
@@ -176,8 +216,7 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "N": N_BLOCKS, "n": BLOCK, "m": NRHS, "shift": SHIFT,
-                   "l2": "host CPU run"},
+        "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": "one full FP64 factor_and_solve of the workload system per step "
                                    "(NumPy oracle restating socu's level loop; BLAS threads = host cores)"},
@@ -190,6 +229,60 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def dmma_peak_tflops(dev):
+    """FP64 tensor-core (DMMA) throughput of this GPU: socu_dmma_peak_launch
+    (register-only mma.sync m8n8k4 f64 chains, 2 CTAs x 256 threads per SM),
+    best of 3 launches timed with CUDA events."""
+    import ctypes
+
+    import torch
+
+    from socu_b200 import _lib
+    lib = _lib.load()
+    sink = torch.zeros(1, dtype=torch.float64, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    st = torch.cuda.current_stream(dev).cuda_stream
+    best = 0.0
+    for _ in range(4):
+        fl = ctypes.c_double(0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        _lib.check(lib.socu_dmma_peak_launch(2 * sms, 256, 20000, sink.data_ptr(), st, ctypes.byref(fl)),
+                   "socu_dmma_peak_launch")
+        b.record()
+        torch.cuda.synchronize(dev)
+        best = max(best, fl.value / (a.elapsed_time(b) * 1e-3) / 1e12)
+    return best
+
+
+def level_counts(N):
+    """Per level: (d, r, l, both) = nodes, nodes with a right / left neighbour, with both."""
+    s, out = 1, []
+    for _ in range(N.bit_length()):
+        d = (N + s) // (2 * s)
+        nodes = [s - 1 + 2 * s * t for t in range(d)]
+        r = sum(1 for i in nodes if i + s < N)
+        lft = sum(1 for i in nodes if i >= s)
+        both = sum(1 for i in nodes if i + s < N and i >= s)
+        out.append((d, r, lft, both))
+        s *= 2
+    return out
+
+
+def node_flops(N, n, m):
+    """Algorithmic flops of the level-node work of a factor_and_solve: potrf
+    n^3/3 per node, trsm n^3 per coupling side, forward step 2 n^2 m per node."""
+    return sum(d * n ** 3 / 3 + (r + lft) * n ** 3 + 2 * d * n * n * m for d, r, lft, _ in level_counts(N))
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -200,7 +293,8 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    L0, E0, b0 = make_problem_gpu(dev)
+    Lh0, Eh0, bh0 = make_problem_host()
+    L0, E0, b0 = Lh0.to(dev), Eh0.to(dev), bh0.to(dev)
     x = torch.zeros_like(b0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 
@@ -219,19 +313,18 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         rounds = max(1, int(mixed.iterations.abs().max()))
         mixed = create_cholesky_refined_solve_launch(L0, E0, b0, x, tol=TOL, max_iter=rounds, use_cuda_graph=False)
-    # plain FP64 factor_and_solve on working copies (in place)
+    # plain FP64 factor_and_solve on working copies (in place); FP64 factor alone
     Lw, Ew, xw = L0.clone(), E0.clone(), b0.clone()
     plain = create_cholesky_factor_and_solve_launch(Lw, Ew, xw, use_cuda_graph=True)
-    # the dominant kernel of the mixed solve: the float backward sweep on a
-    # factor that carries its diagonal inverses (k_bwd<float, resident, inverse>),
-    # one launch per level, timed as whole graph-launched sweeps
+    fac64 = create_cholesky_factor_launch(Lw, Ew, use_cuda_graph=True)
+    # the float backward sweep of the mixed solve (HBM-bound secondary roofline)
     L32, E32 = L0.float(), E0.float()
     create_cholesky_factor_launch(L32, E32, dtype=torch.float32, keep_inverse=True)()
     b32 = b0.float()
     x32 = b32.clone()
-    fac32 = create_cholesky_backward_substitution_launch(L32, E32, x32, dtype=torch.float32, use_cuda_graph=True,
+    bwd32 = create_cholesky_backward_substitution_launch(L32, E32, x32, dtype=torch.float32, use_cuda_graph=True,
                                                          factor_has_inverse=True)
-    sweep_launches = fac32.kernel_count
+    sweep_launches = bwd32.kernel_count
 
     def time_steps(fn, reset, k):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
@@ -247,7 +340,7 @@ def run_ours(args, rank, world, local_rank):
     def reset_plain():
         Lw.copy_(L0); Ew.copy_(E0); xw.copy_(b0)
 
-    def reset_fac():
+    def reset_bwd():
         x32.copy_(b32)
 
     nothing = lambda: None
@@ -257,19 +350,31 @@ def run_ours(args, rank, world, local_rank):
     sampler.__enter__()
     time.sleep(1.5)
     for _ in range(args.warmup):
-        mixed(); reset_plain(); plain(); reset_fac(); fac32()
+        mixed(); reset_plain(); plain(); reset_bwd(); bwd32(); reset_plain(); fac64()
     barrier()
     t_mixed = time_steps(mixed, nothing, args.steps)
     barrier()
     t_plain = time_steps(plain, reset_plain, args.steps)
-    t_fac = time_steps(fac32, reset_fac, args.steps)
+    x_plain = xw.clone()
+    t_fac64 = time_steps(fac64, reset_plain, args.steps)
+    t_bwd = time_steps(bwd32, reset_bwd, args.steps)
     barrier()
 
     eta_dev = float(mixed.eta.max())
     iters = int(mixed.iterations.max())
     eta_check = float(backward_error(L0, E0, x, b0).max())
-    x_plain = xw.clone()
     eta_plain = float(backward_error(L0, E0, x_plain, b0).max())
+    x_mixed = x.clone()
+
+    # per-phase budget: one eager run of each solve with CUDA events around
+    # every kernel (the mixed solve with exactly the rounds the graph ran)
+    prof_mixed = create_cholesky_refined_solve_launch(L0, E0, b0, torch.zeros_like(b0), tol=TOL,
+                                                      max_iter=max(1, abs(iters)), use_cuda_graph=False)
+    reset_plain()
+    phases_plain = plain.profile()
+    phases_mixed = prof_mixed.profile()
+    del prof_mixed
+    dmma_tf = dmma_peak_tflops(dev)
 
     # e2e through the public API with host buffers (pinned), copies inside the timed region
     Lh = L0.cpu().pin_memory(); Eh = E0.cpu().pin_memory(); bh = b0.cpu().pin_memory()
@@ -341,53 +446,83 @@ def run_ours(args, rank, world, local_rank):
     def agg(ts):
         return max_over_ranks(statistics.mean(ts), world, dev)
 
-    sec_mixed, sec_plain, sec_fac, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_fac), agg(t_e2e)
+    sec_mixed, sec_plain, sec_bwd, sec_e2e = agg(t_mixed), agg(t_plain), agg(t_bwd), agg(t_e2e)
+    sec_fac64 = agg(t_fac64)
     sec_e2e_serial = agg(t_e2e_serial)
     del e2e_run, Ld, Ed, bd, xd, Lw, Ew, xw, L32, E32, x32, b32
     torch.cuda.empty_cache()
-    rg = bench_ragged(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
-    ad = bench_autograd(dev, args.steps, time_steps, agg) if not args.skip_ragged else None
+    st = bench_stress(dev, args.steps, time_steps, agg, dmma_tf) if not args.skip_extra else None
+    rg = bench_ragged(dev, args.steps, time_steps, agg, world, rank) if not args.skip_extra else None
+    ad = bench_autograd(dev, args.steps, time_steps, agg) if not args.skip_extra else None
     barrier()
     sampler.__exit__(None, None, None)
     if rank != 0:
         return
     n, N, m = BLOCK, N_BLOCKS, NRHS
     S = storage_len(N)
+    hbm_peak, bf16_peak, peak_src = measured_peaks()
+    # accuracy against LAPACK's banded FP64 Cholesky of the same system
+    Lh_np, Eh_np, bh_np = Lh0[0].numpy(), Eh0[0].numpy(), bh0[0].numpy()
+    x_band = band_solve_fp64(Lh_np, Eh_np, bh_np)
+    fwd_mixed = forward_error(x_mixed[0].cpu().numpy(), x_band)
+    fwd_plain = forward_error(x_plain[0].cpu().numpy(), x_band)
+    # dominant kernel of the mixed solve: the largest share of its profile
+    dom = max(phases_mixed, key=lambda k: phases_mixed[k][0])
+    node_ms, node_launches = phases_mixed["node"]
+    nf = node_flops(N, n, m)
+    node_ach = nf / node_launches / (node_ms * 1e-3 / node_launches) / 1e12
     # algorithmic bytes of one backward sweep: every diagonal block (with its
     # inverse) and every coupling slot read once, x read three times and
     # written once per node, 4-byte floats; per launch = sweep / launches
     sweep_bytes = ((N + S) * n * n + 4.0 * N * n * m) * 4
-    fac_bytes = sweep_bytes / sweep_launches
-    sec_fac = sec_fac / sweep_launches
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    hbm_peak, peak_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        hbm_peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    achieved = fac_bytes / sec_fac / 1e9
+    bwd_ach = sweep_bytes / sweep_launches / (sec_bwd / sweep_launches) / 1e9
+    fac_flops = algorithmic_factor_flops(N, n)
+    fac64_tf = fac_flops / sec_fac64 / 1e12
     cores = len(os.sched_getaffinity(0))
-    cpu_v, cpu_ts = cpu_oracle_solves_per_s(L0[0].cpu().numpy(), E0[0].cpu().numpy(), b0[0].cpu().numpy(), reps=2)
+    cpu_v, cpu_ts = cpu_oracle_solves_per_s(Lh_np, Eh_np, bh_np)
     value = world / sec_mixed
+
+    def budget(ph):
+        return {k: {"ms": round(v[0], 4), "launches": v[1]} for k, v in ph.items()}
+
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec_mixed * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 factor + f64 refinement", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "N": N, "n": n, "m": m, "shift": SHIFT, "tol": TOL,
-                   "max_iter": MAX_ITER, "l2": "256 MB flush before every timed step",
-                   "parallelism": f"replicas x{world} (one system per GPU)"},
+        "config": dict(workload_config(), parallelism=f"replicas x{world} (one system per GPU)"),
         "fp64_plain": {"value": world / sec_plain, "unit": "solves/s", "ms_per_step": sec_plain * 1e3,
-                       "backward_error": eta_plain},
+                       "backward_error": eta_plain, "forward_error": fwd_plain,
+                       "roofline": {"kernel": "FP64 factor (k_node<double> + k_update<double>, graph-launched)",
+                                    "bound": "fp64 tensor (DMMA)", "achieved": fac64_tf, "peak": dmma_tf,
+                                    "unit": "TFLOP/s", "frac": fac64_tf / dmma_tf,
+                                    "peak_source": "measured in this run: socu_dmma_peak_launch (register-only "
+                                                   "mma.sync m8n8k4 f64 chains); the device file has no FP64 figure",
+                                    "algorithmic_flops": fac_flops, "ms": sec_fac64 * 1e3},
+                       "phases": budget(phases_plain)},
         "mixed_over_fp64": sec_plain / sec_mixed,
         "backward_error": {"max": eta_dev, "recomputed": eta_check, "iterations": iters},
-        "factor_flops_fp": algorithmic_factor_flops(N, n),
-        "roofline": {"kernel": "k_bwd<float, resident, inverse> (backward sweep of the mixed solve; "
-                               f"{sweep_launches} launches per sweep, averaged)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "peak_source": peak_src, "traffic": TRAFFIC_BYTES,
-                     "algorithmic_bytes": fac_bytes, "ms_per_launch": sec_fac * 1e3,
-                     "traffic_source": TRAFFIC_NOTE},
+        "forward_error": {"mixed": fwd_mixed, "fp64_plain": fwd_plain,
+                          "reference": "LAPACK banded FP64 Cholesky (scipy solveh_banded) of the same system"},
+        "factor_flops_fp": fac_flops,
+        "phases": dict(budget(phases_mixed), note="one eager run with CUDA events around every kernel, "
+                       f"{abs(iters)} rounds; events add gaps, so the sum exceeds ms_per_step"),
+        "roofline": {"kernel": f"k_node<float> (level nodes of the mixed solve: potrf + coupling solves + forward "
+                               f"step; largest share of the mixed solve: {dom})",
+                     "bound": "tensor", "achieved": node_ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": node_ach / bf16_peak, "peak_source": f"{peak_src} (bf16 dense, MEASURED_PEAKS.json)",
+                     "traffic": NODE_TRAFFIC_BYTES, "traffic_source": NODE_TRAFFIC_NOTE,
+                     "algorithmic_flops_per_launch": nf / node_launches,
+                     "ms_per_launch": node_ms / node_launches},
+        "roofline_sweep": {"kernel": "k_bwd<float, resident, inverse> (backward sweep of the mixed solve; "
+                                     f"{sweep_launches} launches per sweep, averaged)", "bound": "hbm",
+                           "achieved": bwd_ach, "peak": hbm_peak, "unit": "GB/s", "frac": bwd_ach / hbm_peak,
+                           "peak_source": peak_src, "traffic": TRAFFIC_BYTES,
+                           "algorithmic_bytes": sweep_bytes / sweep_launches,
+                           "ms_per_launch": sec_bwd / sweep_launches * 1e3, "traffic_source": TRAFFIC_NOTE},
+        "fp64_dmma_peak_tflops": dmma_tf,
         "cpu_baseline": {"value": cpu_v, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": "one FP64 factor_and_solve of the workload system, median of 2 "
-                                   f"({[round(t, 3) for t in cpu_ts]} s)"},
+                         "sample": f"full FP64 factor_and_solve runs of the workload system for ~{CPU_SAMPLE_S:.0f} s, "
+                                   f"median of {len(cpu_ts)} ({min(cpu_ts):.3f}-{max(cpu_ts):.3f} s)"},
         "e2e": {"value": world / sec_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": sec_e2e * 1e3,
                 "mode": "pipelined: two device buffer sets, copies of neighbouring steps overlap the solve "
@@ -399,8 +534,10 @@ def run_ours(args, rank, world, local_rank):
         # graph run: the prologue holds the first round; the WHILE loop runs the others
         "gpu_launches": (mixed.kernel_count + max(abs(iters) - 1, 0) * mixed.round_kernel_count) * args.steps,
         "clocks": dict(sampler.summary(), window="100 ms samples over all timed regions of this run "
-                                                  "(workload, e2e, ragged) and their warm-ups"),
+                                                  "(workload, e2e, stress, ragged, autograd) and their warm-ups"),
     }
+    if st is not None:
+        line["stress"] = st
     if rg is not None:
         line["ragged"] = rg
     if ad is not None:
@@ -408,19 +545,93 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def bench_ragged(dev, steps, time_steps, agg):
+STRESS_N, STRESS_n, STRESS_m, STRESS_SHIFT, STRESS_SHIFT_LITERAL = 16384, 128, 32, 24.0, 0.05
+
+
+def bench_stress(dev, steps, time_steps, agg, dmma_tf):
+    """Large shape N=16384, n=128, m=32 (~6.4 GB of FP64 blocks): mixed +
+    refinement against the plain FP64 path on the same system.  Shift 24
+    instead of the literal 0.05, at which the README matrix is numerically
+    indefinite (no Cholesky factors it); the literal shift is run once to
+    report the breakdown status of both paths."""
+    import torch
+
+    from socu_b200.block_tridiag_solver import create_cholesky_factor_and_solve_launch, create_cholesky_factor_launch
+    from socu_b200.mixed import backward_error, create_cholesky_refined_solve_launch
+    from socu_b200.problems import readme_blocks
+
+    N, n, m = STRESS_N, STRESS_n, STRESS_m
+    L0, E0, b0 = readme_blocks(N, n, m, shift=STRESS_SHIFT, seed=SEED, batch=1, device=dev)
+    x = torch.zeros_like(b0)
+    mixed = create_cholesky_refined_solve_launch(L0, E0, b0, x, tol=TOL, max_iter=MAX_ITER, use_cuda_graph=True)
+    Lw, Ew, xw = L0.clone(), E0.clone(), b0.clone()
+    plain = create_cholesky_factor_and_solve_launch(Lw, Ew, xw, use_cuda_graph=True)
+    fac64 = create_cholesky_factor_launch(Lw, Ew, use_cuda_graph=True)
+
+    def reset():
+        Lw.copy_(L0); Ew.copy_(E0); xw.copy_(b0)
+
+    mixed(); reset(); plain(); reset(); fac64()
+    torch.cuda.synchronize(dev)
+    k = max(3, steps // 3)
+    t_m = time_steps(mixed, lambda: None, k)
+    t_p = time_steps(plain, reset, k)
+    x_plain = xw.clone()
+    t_f = time_steps(fac64, reset, k)
+    eta_m = float(backward_error(L0, E0, x, b0).max())
+    eta_p = float(backward_error(L0, E0, x_plain, b0).max())
+    fwd = float((x - x_plain).abs().max() / x_plain.abs().max())
+    iters = int(mixed.iterations.max())
+    prof = create_cholesky_refined_solve_launch(L0, E0, b0, torch.zeros_like(b0), tol=TOL,
+                                                max_iter=max(1, abs(iters)), use_cuda_graph=False).profile()
+    sec_m, sec_p, sec_f = agg(t_m), agg(t_p), agg(t_f)
+    fac_flops = algorithmic_factor_flops(N, n)
+    del mixed, plain, fac64, Lw, Ew, xw, L0, E0, b0, x, x_plain
+    torch.cuda.empty_cache()
+    # the literal shift: both paths must report the breakdown rather than a number
+    L1, E1, b1 = readme_blocks(N, n, m, shift=STRESS_SHIFT_LITERAL, seed=SEED, batch=1, device=dev)
+    x1 = torch.zeros_like(b1)
+    brk = create_cholesky_refined_solve_launch(L1, E1, b1, x1, tol=TOL, max_iter=3, use_cuda_graph=False)
+    brk()
+    eta_brk, it_brk = float(brk.eta.max()), int(brk.iterations.min())
+    create_cholesky_factor_and_solve_launch(L1, E1, b1)()
+    finite_plain = bool(torch.isfinite(b1).all())
+    del brk, L1, E1, b1, x1
+    torch.cuda.empty_cache()
+    fac_tf = fac_flops / sec_f / 1e12
+    return {
+        "workload": f"N={N} n={n} m={m} single system, README construction with shift {STRESS_SHIFT:g}",
+        "deviation": f"shift {STRESS_SHIFT_LITERAL:g} (as specified) is numerically indefinite: see breakdown",
+        "mixed_refine": {"value": 1.0 / sec_m, "unit": "solves/s", "ms_per_step": sec_m * 1e3, "eta_max": eta_m,
+                         "iterations": iters, "forward_error_vs_fp64_plain": fwd,
+                         "phases": {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in prof.items()}},
+        "fp64_plain": {"value": 1.0 / sec_p, "unit": "solves/s", "ms_per_step": sec_p * 1e3, "eta_max": eta_p,
+                       "factor_ms": sec_f * 1e3, "factor_tflops": fac_tf, "factor_frac_of_dmma_peak": fac_tf / dmma_tf},
+        "mixed_over_fp64": sec_p / sec_m,
+        "factor_flops": fac_flops,
+        "breakdown_at_literal_shift": {"mixed_eta": eta_brk, "mixed_iterations": it_brk,
+                                       "fp64_solution_finite": finite_plain},
+    }
+
+
+def bench_ragged(dev, steps, time_steps, agg, world=1, rank=0):
     """Uneven MPC-style batch in one persistent launch: FP64 plain and float
-    factor + FP64 refinement.  The packed inputs (several GB) exceed L2."""
+    factor + FP64 refinement.  The packed inputs (several GB) exceed L2.
+    Under several ranks each rank solves its contiguous share of the
+    instances (balanced by factor work, no exchange)."""
     import torch
 
     from socu_b200.problems import fill_ragged, ragged_shapes
     from socu_b200.ragged import (RaggedBatch, create_ragged_factor_and_solve_launch,
-                                  create_ragged_refined_solve_launch)
+                                  create_ragged_refined_solve_launch, shard_instances)
 
     Ns, ns, ms = ragged_shapes(RAGGED_SEED, RAGGED_COUNT)
+    flops = sum(algorithmic_factor_flops(int(N), int(n)) for N, n in zip(Ns, ns))
+    lo, hi = shard_instances(Ns, ns, world, rank)
+    Ns, ns, ms = Ns[lo:hi], ns[lo:hi], ms[lo:hi]
     plain_b = RaggedBatch(Ns, ns, ms, dtype=torch.float64, device=dev)
     L, E, b = plain_b.empty()
-    fill_ragged(plain_b, L, E, b, seed=RAGGED_SEED)
+    fill_ragged(plain_b, L, E, b, seed=RAGGED_SEED + lo)
     mixed_b = RaggedBatch(Ns, ns, ms, dtype=torch.float64, device=dev, refine=True, max_iter=MAX_ITER)
     x = torch.zeros_like(b)
     run_m = create_ragged_refined_solve_launch(mixed_b, L, E, b, x, tol=TOL)
@@ -438,14 +649,23 @@ def bench_ragged(dev, steps, time_steps, agg):
     t_p = time_steps(run_p, reset, k)
     errs = (mixed_b.error_flag(), plain_b.error_flag())
     sec_m, sec_p = agg(t_m), agg(t_p)
-    flops = sum(algorithmic_factor_flops(int(N), int(n)) for N, n in zip(Ns, ns))
+    # per-instance forward error of the mixed solution against the plain FP64 one
+    reset()
+    run_p()
+    sizes = torch.as_tensor(Ns * ns * ms, device=dev)
+    inst = torch.repeat_interleave(torch.arange(len(Ns), device=dev), sizes)
+    dx = torch.zeros(len(Ns), dtype=torch.float64, device=dev).scatter_reduce(0, inst, (x - xw).abs(), "amax")
+    xm = torch.zeros(len(Ns), dtype=torch.float64, device=dev).scatter_reduce(0, inst, xw.abs(), "amax")
+    fwd = float((dx / xm.clamp_min(1e-300)).max())
     out = {
         "workload": RAGGED_WORKLOAD,
         "mixed_refine": {"value": RAGGED_COUNT / sec_m, "unit": "solves/s", "ms_per_step": sec_m * 1e3,
                          "eta_max": float(run_m.eta.max()), "iterations_max": int(run_m.iterations.max()),
-                         "iterations_mean": float(run_m.iterations.double().mean())},
+                         "iterations_mean": float(run_m.iterations.double().mean()),
+                         "forward_error_vs_fp64_plain_max": fwd},
         "fp64_plain": {"value": RAGGED_COUNT / sec_p, "unit": "solves/s", "ms_per_step": sec_p * 1e3,
                        "factor_gflops": flops / sec_p / 1e9},
+        "instances_per_rank": [lo, hi],
         "mixed_over_fp64": sec_p / sec_m,
         "persistent_ctas": plain_b.grid,
         "queue_errors": list(errs),
@@ -491,7 +711,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--skip-ragged", action="store_true", help="omit the ragged-batch and autograd measurements")
+    ap.add_argument("--skip-extra", "--skip-ragged", dest="skip_extra", action="store_true",
+                    help="omit the stress, ragged-batch and autograd measurements")
     ap.add_argument("--profile", action="store_true",
                     help="for profiler runs only: the mixed solve runs without its CUDA graph")
     args = ap.parse_args()

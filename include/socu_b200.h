@@ -127,7 +127,10 @@ int socu_launch_run(socu_launch_t launch, void* stream);
  * 256).  sweep_tensor_cores: float sweeps on inverse-carrying factors use FP64
  * tensor-core (1) or SIMT (2) products.  update_tile: output tile of the
  * blocked Schur update for n > 64 (16 or 32; the reference's block_size).
- * ragged_units: level nodes per task chunk of a ragged batch (1..64). */
+ * ragged_units: level nodes per task chunk of a ragged batch (1..64).
+ * update_tensor_cores: Schur updates of float factors (n <= 128) on the
+ * tcgen05 tensor cores with 3xTF32 operands (1) or on the FP64 / SIMT path (2);
+ * the default takes the tensor cores for n > 64. */
 typedef struct socu_tuning {
   int32_t node_threads;
   int32_t update_threads;
@@ -135,6 +138,7 @@ typedef struct socu_tuning {
   int32_t sweep_tensor_cores;
   int32_t update_tile;
   int32_t ragged_units;
+  int32_t update_tensor_cores;
 } socu_tuning;
 
 /* As socu_launch_create, with per-launch settings (NULL: none) applied on top
@@ -341,6 +345,20 @@ int socu_ragged_destroy(socu_ragged_t batch);
  * the FP64 factor).  `sink` is a device double the kernel may write.  No
  * counterpart in the reference. */
 int socu_dmma_peak_launch(int64_t blocks, int threads, int iters, double* sink, void* stream, double* flops);
+
+/* Error word of the tensor-core (tcgen05) kernels on the current device
+ * (synchronises): 0 ok, 1 a tensor-core wait ran out (that kernel skipped its
+ * result).  reset != 0 clears it afterwards.  No counterpart in the reference. */
+int socu_tc_error(int* flag, int reset);
+
+/* Self-test of the tensor-core (tcgen05) building block of the float path:
+ * one CTA computes D (128 x n_cols) = A (128 x k_depth) * B (n_cols x k_depth)^T
+ * (row-major float arrays) with operands split into TF32 pieces (3xTF32), FP32
+ * accumulation in tensor memory.  n_cols in 16..128 (multiple of 16), k_depth
+ * a multiple of 8.  *error_flag (device int) is set to 1 if a tensor-core wait
+ * ran out.  No counterpart in the reference. */
+int socu_tc_selftest(const float* A, const float* B, float* D, int64_t n_cols, int64_t k_depth, int* error_flag,
+                     void* stream);
 
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */

@@ -45,10 +45,11 @@ class Tuning(ctypes.Structure):
     """socu_tuning: launch settings, 0 = not set (include/socu_b200.h)."""
     _fields_ = [("node_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
                 ("sweep_threads", ctypes.c_int32), ("sweep_tensor_cores", ctypes.c_int32),
-                ("update_tile", ctypes.c_int32), ("ragged_units", ctypes.c_int32)]
+                ("update_tile", ctypes.c_int32), ("ragged_units", ctypes.c_int32),
+                ("update_tensor_cores", ctypes.c_int32)]
 
     FIELDS = ("node_threads", "update_threads", "sweep_threads", "sweep_tensor_cores", "update_tile",
-              "ragged_units")
+              "ragged_units", "update_tensor_cores")
 
     @classmethod
     def from_dict(cls, d):
@@ -114,6 +115,8 @@ _SIGNATURES = {
     "socu_ragged_grid": (_i64, [_vp]),
     "socu_ragged_set_wait_limit": (_int, [_vp, _i64]),
     "socu_ragged_withhold_instance": (_int, [_vp, _i64]),
+    "socu_tc_selftest": (_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp]),
+    "socu_tc_error": (_int, [ctypes.POINTER(_int), _int]),
     "socu_dmma_peak_launch": (_int, [_i64, _int, _int, _vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "socu_ragged_destroy": (_int, [_vp]),
 }

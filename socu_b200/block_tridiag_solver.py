@@ -187,6 +187,20 @@ def _settings(block_dim, block_size):
     return out or None
 
 
+def _profiler(lib, h, sh, dev):
+    """profile() of a launch object: device time per kernel kind of one eager
+    run (CUDA events around every kernel; synchronises), as
+    {kind: (ms, launches)} for the kinds that ran."""
+    def profile():
+        ms = (ctypes.c_double * _lib.KIND_COUNT)()
+        cnt = (ctypes.c_int64 * _lib.KIND_COUNT)()
+        s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
+        with torch.cuda.device(dev):
+            _lib.check(lib.socu_launch_profile(h, s, ms, cnt), "socu_launch_profile")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES) if cnt[i]}
+    return profile
+
+
 def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, settings=None):
     L, E = _as_tensor(L), _as_tensor(E)
     x = _as_tensor(x) if with_x else None
@@ -234,19 +248,10 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, se
         s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
         _lib.check(lib.socu_launch_run(h, s), "socu_launch_run")
 
-    def profile():
-        """Device time per kernel kind of one eager run (CUDA events around
-        every kernel; synchronises): {kind: (ms, launches)}."""
-        ms = (ctypes.c_double * _lib.KIND_COUNT)()
-        cnt = (ctypes.c_int64 * _lib.KIND_COUNT)()
-        s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.socu_launch_profile(h, s, ms, cnt), "socu_launch_profile")
-        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES) if cnt[i]}
-
     callback._socu_arrays = keep
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     callback.uses_cuda_graph = bool(use_cuda_graph)
-    callback.profile = profile
+    callback.profile = _profiler(lib, h, sh, dev)
     callback.settings = dict(settings or {})
     weakref.finalize(callback, lib.socu_launch_destroy, h)
     return callback

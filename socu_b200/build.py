@@ -25,7 +25,7 @@ OUT_DIR = PKG / "lib"
 OUT = OUT_DIR / "libsocu_b200.so"
 STAMP = OUT_DIR / ".build_stamp"
 
-SOURCES = ["capi.cu", "peak.cu"]
+SOURCES = ["capi.cu", "peak.cu", "tc_selftest.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -13,6 +13,7 @@
 #include "../../include/socu_b200.h"
 #include "grad.cuh"
 #include "ragged.cuh"
+#include "tc_update.cuh"
 
 namespace socu {
 namespace {
@@ -174,7 +175,7 @@ bool tuning_valid(const socu_tuning& t) {
   auto thr = [](int v) { return v == 0 || v == 64 || v == 128 || v == 256; };
   return thr(t.node_threads) && thr(t.update_threads) && thr(t.sweep_threads) && t.sweep_tensor_cores >= 0 &&
          t.sweep_tensor_cores <= 2 && (t.update_tile == 0 || t.update_tile == 16 || t.update_tile == 32) &&
-         t.ragged_units >= 0 && t.ragged_units <= 64;
+         t.ragged_units >= 0 && t.ragged_units <= 64 && t.update_tensor_cores >= 0 && t.update_tensor_cores <= 2;
 }
 
 void tuning_merge(socu_tuning* into, const socu_tuning& over) {
@@ -184,6 +185,7 @@ void tuning_merge(socu_tuning* into, const socu_tuning& over) {
   if (over.sweep_tensor_cores) into->sweep_tensor_cores = over.sweep_tensor_cores;
   if (over.update_tile) into->update_tile = over.update_tile;
   if (over.ragged_units) into->ragged_units = over.ragged_units;
+  if (over.update_tensor_cores) into->update_tensor_cores = over.update_tensor_cores;
 }
 
 // Tuned entry for (dtype, n, m), falling back to (dtype, n, any m); zeros if none.
@@ -329,6 +331,9 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   auto fwd_kernel = res ? (inv ? k_fwd<T, true, false, true> : k_fwd<T, true>) : k_fwd<T, false>;
   auto pull_kernel = res ? k_fwd<T, true, true> : k_fwd<T, false, true>;
   auto bwd_kernel = res ? (inv ? k_bwd<T, true, true> : k_bwd<T, true>) : k_bwd<T, false>;
+  // Schur updates of float factors on the tcgen05 tensor cores (3xTF32), on request
+  const bool upd_tc = sizeof(T) == 4 && update_tc_ok(n) && cfg.update_tensor_cores == 1;
+  const size_t su_tc = (size_t)smem_update_tc_bytes(n);
   long long launches = 0;
   const bool run = count == nullptr;
   const int sms = run ? sm_count() : 0;
@@ -340,6 +345,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     if (op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE) {
       e = prepare(node_kernel, sd);
       if (e == cudaSuccess) e = prepare(k_update<T>, su);
+      if (e == cudaSuccess && upd_tc) e = prepare(k_update_tc, su_tc);
     }
     if (e == cudaSuccess) e = prepare(fwd_kernel, ss);
     if (e == cudaSuccess) e = prepare(pull_kernel, ss);
@@ -387,7 +393,15 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
           go_on(fork->aux, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
           cudaEventRecord(fork->join, fork->aux);
         }
-        go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L, upd_thr);
+        if constexpr (sizeof(T) == 4) {
+          if (upd_tc)
+            go_on(st, k_update_tc, SOCU_KIND_UPDATE, (long long)p.B * update_blocks(p.N, L), su_tc, L, 256);
+          else
+            go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L,
+                  upd_thr);
+        } else {
+          go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L, upd_thr);
+        }
         if (forked && pull_blocks > 0)
           cudaStreamWaitEvent(st, fork->join, 0);
         else
@@ -1515,6 +1529,17 @@ int socu_tuning_get(socu_dtype dtype, int64_t n, int64_t n_rhs, socu_tuning* out
     return SOCU_ERR_INVALID_ARGUMENT;
   *out = tuning_lookup(dtype, (int)n, (int)n_rhs);
   return SOCU_OK;
+}
+
+int socu_tc_error(int* flag, int reset) {
+  if (flag == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *flag = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(flag, g_tc_error, sizeof(int));
+  if (e == cudaSuccess && reset) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int));
+  }
+  return cuda_status(e);
 }
 
 int socu_tuning_clear(void) {

@@ -1,0 +1,167 @@
+// Schur update and fill-in of one factor level for FLOAT blocks (n <= 128)
+// on the tcgen05 tensor cores (tc_gemm.cuh: 3xTF32 split, FP32 accumulation
+// in tensor memory).  Same tasks and results layout as update_full_body
+// (nd_kernels.cuh): task u-1 < U updates target j = 2su-1 completely,
+//     L_j -= F F^T + G^T G          (lower triangle; F = E[o_l+2u-2], G = E[o_l+2u-1])
+// as one product D = A A^T with A = [F | G^T] (n x 2n), and task U + t-1
+// forms the fill-in of node t,
+//     X = E[o_{l+1}+t-1] -= F G     (F = E[o_l+2t], G = E[o_l+2t-1])
+// as D = F (G^T)^T.  (socu: syrk K5/K6 and gemm K7,
+// socu/block_tridiag_solver.py:282-377, socu/blas/syrk.py, socu/blas/gemm.py;
+// the reference accumulates the two syrk contributions with atomics, here each
+// output block has one writer.)
+//
+// The MMA is M = 128 rows (rows n..127 of A are zero), N = n rounded up to 16
+// columns, K streamed in chunks of kTcKC columns through one shared buffer:
+// stage (TF32 split, 8 rows x 4 columns per 32 threads: conflict-free) ->
+// fence -> barrier -> one thread issues 3 kTcKC/8 MMAs and commits to an
+// mbarrier -> everyone waits (bounded) -> next chunk.  The epilogue reads the
+// accumulator from TMEM (warp w: rows 32 (w % 4).., column half w / 4) and
+// subtracts it from the block in global memory.
+#pragma once
+
+#include "nd_kernels.cuh"
+#include "tc_gemm.cuh"
+
+namespace socu {
+
+constexpr int kTcKC = 32;                                  // K columns per staged chunk
+constexpr unsigned long long kTcWaitNs = 200000000ull;    // bound of one tensor-core wait (0.2 s)
+constexpr int kTcMaxN = 128;
+
+__host__ __device__ inline int tc_ncols(int n) { return ((n + 15) / 16) * 16; }
+// shared memory: A hi/lo planes (128 x kTcKC) + B hi/lo planes (N x kTcKC)
+__host__ __device__ inline long long smem_update_tc_bytes(int n) {
+  return 2LL * 128 * kTcKC * 4 + 2LL * tc_ncols(n) * kTcKC * 4;
+}
+__host__ __device__ inline bool update_tc_ok(int n) { return n >= 1 && n <= kTcMaxN; }
+
+// Error word of the tensor-core kernels (1: a wait ran out); one per device.
+__device__ int g_tc_error;
+
+// Stage columns [k0, k0 + kTcKC) of a rows x K operand into hi/lo planes.
+// val(r, k) gives the element (only called for r < rows, k < K); the rest is 0.
+template <class Val>
+__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int rows_pad, int rows, int K,
+                                         int k0, Val val) {
+  constexpr int kq = kTcKC / 4;                        // 4-column groups per chunk
+  const int units = (rows_pad / 8) * kq;               // 8 x 4 units
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int u = warp; u < units; u += nw) {
+    const int r = (u / kq) * 8 + (lane >> 2);
+    const int kk = (u % kq) * 4 + (lane & 3);
+    const int k = k0 + kk;
+    const float v = (r < rows && k < K) ? val(r, k) : 0.0f;
+    tc::put_split(hi, lo, r, kk, kTcKC, v);
+  }
+}
+
+// One update task (see the file comment), all threads of the CTA (multiple
+// of 128).  tmem: 128-column accumulator of this CTA; bar: its mbarrier,
+// phase counter in *phase (the caller keeps it across tasks).
+__device__ __forceinline__ void update_tc_body(const Problem<float>& p, const Level& lv, int b, int task,
+                                               unsigned char* smem, uint32_t tmem, uint64_t* bar,
+                                               unsigned* phase) {
+  const int n = p.n, N = p.N, s = lv.s;
+  const int U = N / (2 * s);
+  const int nc = tc_ncols(n);
+  unsigned char* a_hi = smem;
+  unsigned char* a_lo = a_hi + 128 * kTcKC * 4;
+  unsigned char* b_hi = a_lo + 128 * kTcKC * 4;
+  unsigned char* b_lo = b_hi + nc * kTcKC * 4;
+  const bool target = task < U;
+  const float *F, *G;
+  float* Out;
+  int K;
+  if (target) {
+    const int u = task + 1, j = 2 * s * u - 1;
+    F = p.Eb(b, lv.oc + 2 * (u - 1));
+    G = j + s < N ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
+    Out = p.Lb(b, j);
+    K = G ? 2 * n : n;
+  } else {
+    const int t = task - U + 1, i = s - 1 + 2 * s * t;
+    if (i + s >= N) return;
+    F = p.Eb(b, lv.oc + 2 * t);
+    G = p.Eb(b, lv.oc + 2 * t - 1);
+    Out = p.Eb(b, lv.on + t - 1);
+    K = n;
+  }
+  bool ok;
+  for (int k0 = 0; k0 < K; k0 += kTcKC) {
+    // A = [F | G^T] (target) or F (fill-in): A(r, k) = k < n ? F[r][k] : G[k-n][r]
+    tc_stage(a_hi, a_lo, 128, n, K, k0, [&](int r, int k) {
+      return k < n ? F[(long long)r * n + k] : G[(long long)(k - n) * n + r];
+    });
+    // fill-in: B(c, k) = G[k][c]; targets use B = A (its first nc rows)
+    if (!target) tc_stage(b_hi, b_lo, nc, n, K, k0, [&](int c, int k) { return G[(long long)k * n + c]; });
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0) {
+      const uint32_t ah = tc::saddr(a_hi), al = tc::saddr(a_lo);
+      const uint32_t bh = target ? ah : tc::saddr(b_hi), bl = target ? al : tc::saddr(b_lo);
+      tc::gemm_3xtf32(tmem, ah, al, bh, bl, nc, kTcKC, k0 > 0 ? 1u : 0u);
+      tc::commit(bar);
+    }
+    // every thread waits for the chunk's MMAs before the buffer is restaged;
+    // the vote keeps the CTA's control flow uniform if a wait runs out
+    const bool done = tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+    ok = __syncthreads_and(done) != 0;
+    tc::fence_after_sync();
+    if (!ok) {
+      // second bound for MMAs still in flight before the caller frees TMEM
+      tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+      if (threadIdx.x == 0) atomicExch(&g_tc_error, 1);
+      *phase += 1;
+      return;
+    }
+    *phase += 1;
+  }
+  // epilogue: Out -= D (lower triangle for targets)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3, halves = blockDim.x / 128, h = warp >> 2;
+  const int r = 32 * q + lane;
+  const int span = ((nc / 8 + halves - 1) / halves) * 8;
+  const int c_begin = h * span, c_end = min(nc, c_begin + span);
+  for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+    if (target && c0 > 32 * q + 31) break;   // warp-uniform: every column above this warp's rows
+    if (32 * q >= n) break;
+    float v[8];
+    tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+    tc::tmem_wait_ld();
+    if (r < n) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int c = c0 + i;
+        if (c < n && (!target || c <= r)) Out[(long long)r * n + c] -= v[i];
+      }
+    }
+  }
+}
+
+// One CTA per update task of one level (grid = B x update_blocks).
+__global__ void __launch_bounds__(256, 1) k_update_tc(Problem<float> p, Level lv) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  const int per_b = update_blocks(p.N, lv);
+  const int b = blockIdx.x / per_b;
+  const int task = blockIdx.x - b * per_b;
+  if (!p.active(b)) return;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) tc::tmem_alloc(&tbase, 128);
+  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  unsigned phase = 0;
+  update_tc_body(p, lv, b, task, smem_raw, tbase, &bar, &phase);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tbase, 128);
+}
+
+}  // namespace socu

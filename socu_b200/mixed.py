@@ -21,7 +21,7 @@ import weakref
 import torch
 
 from . import _lib
-from .block_tridiag_solver import _as_tensor, _stream_handle, _validate
+from .block_tridiag_solver import _as_tensor, _profiler, _stream_handle, _validate
 
 __all__ = ["create_cholesky_refined_solve_launch", "block_tridiag_residual", "backward_error"]
 
@@ -94,6 +94,8 @@ def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_i
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     # graph mode: the refinement rounds run in a conditional WHILE node
     callback.round_kernel_count = int(lib.socu_launch_round_kernel_count(h))
+    # eager run with per-kernel events (all max_iter rounds; not the graph)
+    callback.profile = _profiler(lib, h, sh, dev)
     weakref.finalize(callback, lib.socu_launch_destroy, h)
     return callback
 

@@ -1,0 +1,64 @@
+"""The tcgen05 tensor-core building block of the float path (needs a B200).
+
+socu_tc_selftest runs one CTA through the same staging (TF32 hi/lo split into
+the K-major core-matrix layout), shared-memory and instruction descriptors,
+tcgen05.mma issue, commit-to-mbarrier and tensor-memory loads as the solver's
+tensor-core kernels.  D = A B^T must match an FP64 product to FP32 accuracy
+(3xTF32: relative error ~1e-6 of |A| |B|), with no wait running out.
+"""
+import pytest
+import torch
+
+from socu_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("N,K", [(16, 8), (64, 64), (128, 64), (64, 128), (32, 200)])
+def test_tc_gemm_matches_fp64(N, K):
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(N * 1000 + K)
+    A = torch.randn(128, K, device="cuda", generator=g)
+    B = torch.randn(N, K, device="cuda", generator=g)
+    D = torch.full((128, N), float("nan"), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = lib.socu_tc_selftest(A.data_ptr(), B.data_ptr(), D.data_ptr(), N, K, err.data_ptr(),
+                              torch.cuda.current_stream().cuda_stream)
+    assert st == 0, lib.socu_status_string(st)
+    torch.cuda.synchronize()
+    assert int(err) == 0
+    ref = A.double() @ B.double().T
+    scale = (A.double().abs() @ B.double().abs().T)
+    rel = float(((D.double() - ref).abs() / scale).max())
+    assert rel <= 2e-5, rel   # FP32 accumulation over K terms; one TF32 pass would give ~1e-3
+    # a single TF32 pass would be ~1e-3 off: the split really runs
+    assert torch.isfinite(D).all()
+
+
+@pytest.mark.parametrize("n", [16, 48, 64, 68, 100, 128])
+@pytest.mark.parametrize("op", ["factor_and_solve", "factor+solve"])
+def test_tc_update_parity(n, op):
+    """Float factor with the Schur updates on the tensor cores (update_tensor_cores=1)
+    against the oracle at the reference's float tolerance, no wait running out."""
+    import numpy as np
+
+    from oracle import generators, nd_cholesky as nd
+    from socu_b200.block_tridiag_solver import _launch_with_settings
+
+    N = 21
+    L_np, E_np, b_np = generators.readme_problem(N, n, 3, shift=10.0 + 2.0 * np.sqrt(n), seed=n)
+    _, _, x_ref = nd.nd_factor_and_solve(L_np, E_np, b_np)
+    L, E, x = (torch.tensor(a, dtype=torch.float32, device="cuda") for a in (L_np, E_np, b_np))
+    settings = {"update_tensor_cores": 1}
+    if op == "factor_and_solve":
+        _launch_with_settings("factor_and_solve", L, E, x, torch.float32, settings)()
+    else:
+        _launch_with_settings("factor", L, E, None, torch.float32, settings)()
+        _launch_with_settings("solve", L, E, x, torch.float32, settings)()
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    import ctypes
+    flag = ctypes.c_int(0)
+    assert lib.socu_tc_error(ctypes.byref(flag), 1) == 0 and flag.value == 0
+    rel = np.abs(x.double().cpu().numpy() - x_ref[0]).max() / np.abs(x_ref).max()
+    assert rel < 1e-4, rel
