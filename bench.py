@@ -582,8 +582,12 @@ def bench_stress(dev, steps, time_steps, agg, dmma_tf):
     eta_p = float(backward_error(L0, E0, x_plain, b0).max())
     fwd = float((x - x_plain).abs().max() / x_plain.abs().max())
     iters = int(mixed.iterations.max())
-    prof = create_cholesky_refined_solve_launch(L0, E0, b0, torch.zeros_like(b0), tol=TOL,
-                                                max_iter=max(1, abs(iters)), use_cuda_graph=False).profile()
+    try:
+        prof = create_cholesky_refined_solve_launch(L0, E0, b0, torch.zeros_like(b0), tol=TOL,
+                                                    max_iter=max(1, abs(iters)), use_cuda_graph=False).profile()
+        phases = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in prof.items()}
+    except RuntimeError as exc:   # the budget is a diagnostic: report instead of failing the line
+        phases = {"error": str(exc)}
     sec_m, sec_p, sec_f = agg(t_m), agg(t_p), agg(t_f)
     fac_flops = algorithmic_factor_flops(N, n)
     del mixed, plain, fac64, Lw, Ew, xw, L0, E0, b0, x, x_plain
@@ -604,7 +608,7 @@ def bench_stress(dev, steps, time_steps, agg, dmma_tf):
         "deviation": f"shift {STRESS_SHIFT_LITERAL:g} (as specified) is numerically indefinite: see breakdown",
         "mixed_refine": {"value": 1.0 / sec_m, "unit": "solves/s", "ms_per_step": sec_m * 1e3, "eta_max": eta_m,
                          "iterations": iters, "forward_error_vs_fp64_plain": fwd,
-                         "phases": {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in prof.items()}},
+                         "phases": phases},
         "fp64_plain": {"value": 1.0 / sec_p, "unit": "solves/s", "ms_per_step": sec_p * 1e3, "eta_max": eta_p,
                        "factor_ms": sec_f * 1e3, "factor_tflops": fac_tf, "factor_frac_of_dmma_peak": fac_tf / dmma_tf},
         "mixed_over_fp64": sec_p / sec_m,

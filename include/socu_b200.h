@@ -105,6 +105,17 @@ int socu_cholesky_solve(socu_dtype dtype, const void* L, const void* E, void* x,
 int socu_cholesky_run(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask, int64_t batch,
                       int64_t horizon, int64_t n, int64_t n_rhs, void* stream);
 
+/* As socu_cholesky_run for the two factor ops (and SOCU_OP_FACTOR_INV), with a
+ * per-instance numerical status: info (batch,) device int32, set to 0 for
+ * every batch entry, then to 1 + i for entries whose factorisation failed,
+ * i the first failing node in elimination order (lowest separator level,
+ * then lowest block index): a pivot <= 0 (the Schur-complemented block is not
+ * positive definite) or a non-finite value.  Blocks of a failed entry hold
+ * non-finite values afterwards.  No counterpart in the reference, whose
+ * potrf takes the square root of any pivot (socu/blas/potrf.py:97-117). */
+int socu_cholesky_run_info(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask,
+                           int32_t* info, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream);
+
 /* Recorded launches bound to fixed buffers, optionally captured once into a
  * CUDA graph at creation (the recorded launches + create_cuda_graph_callback
  * of socu/block_tridiag_solver.py:784-790 and socu/utils.py:39-65).  The mask
@@ -129,8 +140,9 @@ int socu_launch_run(socu_launch_t launch, void* stream);
  * blocked Schur update for n > 64 (16 or 32; the reference's block_size).
  * ragged_units: level nodes per task chunk of a ragged batch (1..64).
  * update_tensor_cores: Schur updates of float factors (n <= 128) on the
- * tcgen05 tensor cores with 3xTF32 operands (1) or on the FP64 / SIMT path (2);
- * the default takes the tensor cores for n > 64. */
+ * tcgen05 tensor cores with 3xTF32 operands (1) or on the FP64 / SIMT path (2).
+ * node_tensor_cores: the coupling and forward products of float level nodes
+ * (n <= 64, 2n + n_rhs <= 256) on the tcgen05 tensor cores (1) or SIMT (2). */
 typedef struct socu_tuning {
   int32_t node_threads;
   int32_t update_threads;
@@ -139,6 +151,7 @@ typedef struct socu_tuning {
   int32_t update_tile;
   int32_t ragged_units;
   int32_t update_tensor_cores;
+  int32_t node_tensor_cores;
 } socu_tuning;
 
 /* As socu_launch_create, with per-launch settings (NULL: none) applied on top
@@ -147,6 +160,13 @@ typedef struct socu_tuning {
 int socu_launch_create_tuned(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
                              const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                              int use_cuda_graph, const socu_tuning* settings, void* stream);
+
+/* As socu_launch_create_tuned, with the per-instance factor status of
+ * socu_cholesky_run_info (info may be NULL; non-NULL only for the factor ops),
+ * rewritten by every run. */
+int socu_launch_create_ex(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
+                          const uint8_t* mask, int32_t* info, int64_t batch, int64_t horizon, int64_t n,
+                          int64_t n_rhs, int use_cuda_graph, const socu_tuning* settings, void* stream);
 
 /* Install (settings != NULL) or remove the tuned entry for (dtype, n, n_rhs);
  * n_rhs = 0 is the entry for any n_rhs without one of its own.  Launches
@@ -181,6 +201,11 @@ typedef enum socu_kernel_kind {
  * refined solve runs all its max_iter rounds.  For measurement only: the
  * events add gaps between kernels. */
 int socu_launch_profile(socu_launch_t launch, void* stream, double* ms, int64_t* launches);
+
+/* After a failed socu_launch_profile in this thread: the kernel kind of the
+ * launch the error was charged to (-1 if none) and whether the error was
+ * already pending before that launch (0) or raised by it (1). */
+int socu_profile_error(int* kind, int* where);
 
 /* Number of kernels one run enqueues (0 for a NULL launch).  For a
  * graph-captured refined solve: the kernels before the refinement loop. */
@@ -352,13 +377,15 @@ int socu_dmma_peak_launch(int64_t blocks, int threads, int iters, double* sink, 
 int socu_tc_error(int* flag, int reset);
 
 /* Self-test of the tensor-core (tcgen05) building block of the float path:
- * one CTA computes D (128 x n_cols) = A (128 x k_depth) * B (n_cols x k_depth)^T
- * (row-major float arrays) with operands split into TF32 pieces (3xTF32), FP32
- * accumulation in tensor memory.  n_cols in 16..128 (multiple of 16), k_depth
- * a multiple of 8.  *error_flag (device int) is set to 1 if a tensor-core wait
- * ran out.  No counterpart in the reference. */
-int socu_tc_selftest(const float* A, const float* B, float* D, int64_t n_cols, int64_t k_depth, int* error_flag,
-                     void* stream);
+ * one CTA computes D = A (m_rows x k_depth) * B (n_cols x k_depth)^T
+ * (row-major float arrays; m_rows 64 or 128) with operands split into TF32
+ * pieces (3xTF32), FP32 accumulation in tensor memory, and writes the
+ * accumulator as it lies in tensor memory: D is (128 x n_cols), row t = TMEM
+ * lane t.  n_cols in 16..128 (multiple of 16), k_depth a multiple of 8.
+ * *error_flag (device int) is set to 1 if a tensor-core wait ran out.  No
+ * counterpart in the reference. */
+int socu_tc_selftest(const float* A, const float* B, float* D, int64_t m_rows, int64_t n_cols, int64_t k_depth,
+                     int* error_flag, void* stream);
 
 /* r = b - Psi x in FP64 against the original blocks (no counterpart in the
  * reference).  L and E as for the factor input (lower(L_i), level-0 slots). */

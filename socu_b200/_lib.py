@@ -46,10 +46,10 @@ class Tuning(ctypes.Structure):
     _fields_ = [("node_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
                 ("sweep_threads", ctypes.c_int32), ("sweep_tensor_cores", ctypes.c_int32),
                 ("update_tile", ctypes.c_int32), ("ragged_units", ctypes.c_int32),
-                ("update_tensor_cores", ctypes.c_int32)]
+                ("update_tensor_cores", ctypes.c_int32), ("node_tensor_cores", ctypes.c_int32)]
 
     FIELDS = ("node_threads", "update_threads", "sweep_threads", "sweep_tensor_cores", "update_tile",
-              "ragged_units", "update_tensor_cores")
+              "ragged_units", "update_tensor_cores", "node_tensor_cores")
 
     @classmethod
     def from_dict(cls, d):
@@ -85,10 +85,14 @@ _SIGNATURES = {
     "socu_launch_run": (_int, [_vp, _vp]),
     "socu_launch_create_tuned": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p,
                                         _i64, _i64, _i64, _i64, _int, _vp, _vp]),
+    "socu_launch_create_ex": (_int, [ctypes.POINTER(_vp), _int, _int, _vp, _vp, _vp, _u8p, _vp,
+                                     _i64, _i64, _i64, _i64, _int, _vp, _vp]),
+    "socu_cholesky_run_info": (_int, [_int, _int, _vp, _vp, _vp, _u8p, _vp, _i64, _i64, _i64, _i64, _vp]),
     "socu_tuning_set": (_int, [_int, _i64, _i64, _vp]),
     "socu_tuning_get": (_int, [_int, _i64, _i64, _vp]),
     "socu_tuning_clear": (_int, []),
     "socu_launch_profile": (_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i64)]),
+    "socu_profile_error": (_int, [ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "socu_launch_kernel_count": (_i64, [_vp]),
     "socu_launch_round_kernel_count": (_i64, [_vp]),
     "socu_launch_destroy": (_int, [_vp]),
@@ -115,7 +119,7 @@ _SIGNATURES = {
     "socu_ragged_grid": (_i64, [_vp]),
     "socu_ragged_set_wait_limit": (_int, [_vp, _i64]),
     "socu_ragged_withhold_instance": (_int, [_vp, _i64]),
-    "socu_tc_selftest": (_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp]),
+    "socu_tc_selftest": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _vp, _vp]),
     "socu_tc_error": (_int, [ctypes.POINTER(_int), _int]),
     "socu_dmma_peak_launch": (_int, [_i64, _int, _int, _vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "socu_ragged_destroy": (_int, [_vp]),

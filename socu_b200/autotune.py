@@ -14,6 +14,8 @@ Settings (``socu_tuning``; 0 = built-in heuristic):
                          tensor-core products, 2 SIMT row dots
     update_tile          output tile of the blocked Schur update (n > 64): 16, 32
     ragged_units         level nodes per task chunk of a ragged batch: 1..64
+    update_tensor_cores  Schur updates of float factors (n <= 128) on the
+                         tcgen05 tensor cores, 3xTF32 (1), or not (2)
 
 Search: coordinate descent from the built-in heuristics.  Each knob in turn
 is tried at every value with the others held at the best so far; a candidate
@@ -45,13 +47,15 @@ from . import _lib
 __all__ = ["cache_path", "load_cache", "save_entry", "tune", "candidates", "current_settings", "install",
            "KNOBS", "maybe_autotune"]
 
-KNOBS = ("node_threads", "sweep_tensor_cores", "sweep_threads", "update_threads", "update_tile")
+KNOBS = ("update_tensor_cores", "node_threads", "sweep_tensor_cores", "sweep_threads", "update_threads",
+         "update_tile")
 _VALUES = {
     "node_threads": (0, 64, 128, 256),
     "update_threads": (0, 128, 256),
     "sweep_threads": (0, 64, 128, 256),
     "sweep_tensor_cores": (0, 1, 2),
     "update_tile": (0, 16, 32),
+    "update_tensor_cores": (0, 1, 2),
 }
 _loaded = set()
 _tuned = set()
@@ -152,6 +156,8 @@ def candidates(n: int, n_rhs: int, dtype) -> dict:
         if k == "update_tile" and n <= 64:
             continue
         if k == "sweep_tensor_cores" and (n > 64 or _dtype_name(dtype) == "float64"):
+            continue
+        if k == "update_tensor_cores" and (n > 128 or _dtype_name(dtype) == "float64"):
             continue
         out[k] = vals
     return out

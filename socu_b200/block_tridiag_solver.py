@@ -196,12 +196,25 @@ def _profiler(lib, h, sh, dev):
         cnt = (ctypes.c_int64 * _lib.KIND_COUNT)()
         s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
         with torch.cuda.device(dev):
-            _lib.check(lib.socu_launch_profile(h, s, ms, cnt), "socu_launch_profile")
+            status = lib.socu_launch_profile(h, s, ms, cnt)
+        if status != _lib.SOCU_OK:
+            kind, where = ctypes.c_int(-1), ctypes.c_int(-1)
+            lib.socu_profile_error(ctypes.byref(kind), ctypes.byref(where))
+            name = _lib.KIND_NAMES[kind.value] if 0 <= kind.value < _lib.KIND_COUNT else "none"
+            _lib.check(status, f"socu_launch_profile (at a {name} launch, "
+                               f"{'raised by it' if where.value == 1 else 'pending before it'})")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES) if cnt[i]}
     return profile
 
 
-def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, settings=None):
+def _check_info(info, batch, dev):
+    assert isinstance(info, torch.Tensor), "info must be a torch tensor"
+    assert info.dtype == torch.int32 and info.ndim == 1 and info.shape[0] == batch, \
+        "info must be an int32 tensor of shape (batch_dim,)"
+    assert info.device == dev and info.is_contiguous(), "info must be a contiguous tensor on the solver's device"
+
+
+def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, settings=None, info=None):
     L, E = _as_tensor(L), _as_tensor(E)
     x = _as_tensor(x) if with_x else None
     mask = _as_tensor(mask) if mask is not None else None
@@ -223,6 +236,8 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, se
         assert a.device == dev, f"{name} must be on {dev}"
     if mask is not None:
         assert mask.device == dev and mask.is_contiguous(), "mask must be a contiguous array on the solver's device"
+    if info is not None:
+        _check_info(info, batch, dev)
 
     lib = _lib.load()
     from . import autotune
@@ -233,15 +248,16 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, se
     tuning = _lib.Tuning.from_dict(settings) if settings else None
     with torch.cuda.device(dev):
         cap_stream = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
-        status = lib.socu_launch_create_tuned(
+        status = lib.socu_launch_create_ex(
             ctypes.byref(handle), op, dt,
             L.data_ptr(), E.data_ptr() if E.numel() else None,
             x.data_ptr() if with_x else None,
             mask.data_ptr() if mask is not None else None,
+            info.data_ptr() if info is not None else None,
             batch, horizon, n, n_rhs, int(bool(use_cuda_graph)),
             ctypes.byref(tuning) if tuning is not None else None, cap_stream)
     _lib.check(status, "socu_launch_create")
-    keep = (L, E, x, mask)
+    keep = (L, E, x, mask, info)
     h = handle.value
 
     def callback():
@@ -275,22 +291,28 @@ def _launch_with_settings(op, L, E, x, dtype, settings, use_cuda_graph=True):
 
 def create_cholesky_factor_launch(L, E, mask=None, block_dim=None, block_size=None,
                                   dtype=torch.float64, device=None, stream=None,
-                                  use_cuda_graph=False, *, keep_inverse=False):
+                                  use_cuda_graph=False, *, keep_inverse=False, info=None):
     """In-place ND Cholesky factor of (L, E); returns a zero-argument callable.
 
     keep_inverse (extension, n <= 64): also store W_i^T = C_i^{-T} in the strict
-    upper triangle of every L_i, for the ``factor_has_inverse`` sweeps."""
+    upper triangle of every L_i, for the ``factor_has_inverse`` sweeps.
+    info (extension): int32 tensor (batch_dim,) on the device, rewritten by every
+    call: 0 where the factorisation succeeded, else 1 + the first failing node
+    (lowest separator level, then lowest block index) whose pivot was not
+    positive (the reference has no numerical status)."""
     op = _lib.OP_FACTOR_INV if keep_inverse else _lib.OP_FACTOR
     return _create(op, L, E, None, mask, dtype, device, stream, use_cuda_graph, False,
-                   _settings(block_dim, block_size))
+                   _settings(block_dim, block_size), info)
 
 
 def create_cholesky_factor_and_solve_launch(L, E, x, mask=None, block_dim=None, block_size=None,
                                             dtype=torch.float64, device=None, stream=None,
-                                            use_cuda_graph=False):
-    """Factor fused with the forward sweep, then the backward sweep; x: b in, solution out."""
+                                            use_cuda_graph=False, *, info=None):
+    """Factor fused with the forward sweep, then the backward sweep; x: b in, solution out.
+
+    info (extension): per-instance factor status, as for create_cholesky_factor_launch."""
     return _create(_lib.OP_FACTOR_AND_SOLVE, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
-                   _settings(block_dim, block_size))
+                   _settings(block_dim, block_size), info)
 
 
 def create_cholesky_forward_substitution_launch(L, E, x, mask=None, block_dim=None, block_size=None,

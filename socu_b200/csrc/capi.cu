@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -49,6 +50,7 @@ void schedule(int N, Schedule* out) {
     lv.op = prev;
     lv.tc = 0;
     lv.tile = kTile;
+    lv.pre = 0;
     s *= 2;
     prev = curr;
     curr = nxt;
@@ -88,7 +90,9 @@ int g_n_prepared = 0;
 
 template <typename K>
 cudaError_t prepare(K kernel, size_t smem) {
-  if (smem <= 48 * 1024) return cudaSuccess;
+  // the default limit (48 KB) covers dynamic plus static shared memory; keep a
+  // margin for the kernels' static __shared__ words
+  if (smem <= 40 * 1024) return cudaSuccess;
   int dev = 0;
   cudaGetDevice(&dev);
   const void* fn = reinterpret_cast<const void*>(kernel);
@@ -131,7 +135,10 @@ int occupancy(K kernel, int dev, int threads, size_t smem) {
     if (g_occ[i].fn == fn && g_occ[i].dev == dev && g_occ[i].smem == smem && g_occ[i].threads == threads)
       return g_occ[i].blocks;
   int v = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess) v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess) {
+    v = 0;
+    (void)cudaGetLastError();   // the fallback path handles it; do not leave the error pending
+  }
   if (g_n_occ < kCacheSlots) g_occ[g_n_occ++] = OccSlot{fn, dev, smem, threads, v};
   return v;
 }
@@ -175,7 +182,8 @@ bool tuning_valid(const socu_tuning& t) {
   auto thr = [](int v) { return v == 0 || v == 64 || v == 128 || v == 256; };
   return thr(t.node_threads) && thr(t.update_threads) && thr(t.sweep_threads) && t.sweep_tensor_cores >= 0 &&
          t.sweep_tensor_cores <= 2 && (t.update_tile == 0 || t.update_tile == 16 || t.update_tile == 32) &&
-         t.ragged_units >= 0 && t.ragged_units <= 64 && t.update_tensor_cores >= 0 && t.update_tensor_cores <= 2;
+         t.ragged_units >= 0 && t.ragged_units <= 64 && t.update_tensor_cores >= 0 && t.update_tensor_cores <= 2 &&
+         t.node_tensor_cores >= 0 && t.node_tensor_cores <= 2;
 }
 
 void tuning_merge(socu_tuning* into, const socu_tuning& over) {
@@ -186,6 +194,7 @@ void tuning_merge(socu_tuning* into, const socu_tuning& over) {
   if (over.update_tile) into->update_tile = over.update_tile;
   if (over.ragged_units) into->ragged_units = over.ragged_units;
   if (over.update_tensor_cores) into->update_tensor_cores = over.update_tensor_cores;
+  if (over.node_tensor_cores) into->node_tensor_cores = over.node_tensor_cores;
 }
 
 // Tuned entry for (dtype, n, m), falling back to (dtype, n, any m); zeros if none.
@@ -211,7 +220,11 @@ struct Prof {
   std::vector<cudaEvent_t> start, stop;
   std::vector<int> kind;
   cudaError_t err = cudaSuccess;
+  int err_kind = -1;    // kernel kind of the first failing launch
+  int err_where = -1;   // 0: error pending before that launch, 1: raised by it
 };
+// kind and place of the last profiling failure in this thread (socu_profile_error)
+thread_local int g_prof_err_kind = -1, g_prof_err_where = -1;
 thread_local Prof* g_prof = nullptr;
 
 void prof_mark(cudaStream_t s, bool begin, int kind) {
@@ -231,8 +244,61 @@ void prof_mark(cudaStream_t s, bool begin, int kind) {
     g_prof->stop.push_back(e);
   }
 }
-inline void prof_begin(cudaStream_t s, int kind) { prof_mark(s, true, kind); }
-inline void prof_end(cudaStream_t s) { prof_mark(s, false, 0); }
+inline void prof_begin(cudaStream_t s, int kind) {
+  if (g_prof == nullptr) return;
+  // a launch error must be charged to the launch that caused it
+  const cudaError_t prev = cudaGetLastError();
+  if (prev != cudaSuccess && g_prof->err == cudaSuccess) {
+    g_prof->err = prev;
+    g_prof->err_kind = kind;
+    g_prof->err_where = 0;
+  }
+  prof_mark(s, true, kind);
+}
+inline void prof_end(cudaStream_t s) {
+  if (g_prof == nullptr) return;
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess && g_prof->err == cudaSuccess) {
+    g_prof->err = e;
+    g_prof->err_kind = g_prof->kind.empty() ? -1 : g_prof->kind.back();
+    g_prof->err_where = 1;
+  }
+  prof_mark(s, false, 0);
+}
+
+// Programmatic dependent launch of a kernel that follows another kernel of the
+// same op on the same stream: it may start while its predecessor finishes and
+// waits (griddepcontrol.wait in the kernel) before it reads the predecessor's
+// results.  The first kernel of an op is launched plainly, so it is fully
+// ordered after whatever the caller enqueued before.  SOCU_PDL=0 turns
+// programmatic launches off.
+bool pdl_enabled() {
+  static const int on = [] {
+    const char* v = std::getenv("SOCU_PDL");
+    return (v != nullptr && v[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
+template <typename... KArgs, typename... Args>
+void launch(void (*kernel)(KArgs...), unsigned blocks, unsigned threads, size_t smem, cudaStream_t s, bool pdl,
+            Args... args) {
+  if (!pdl || !pdl_enabled()) {
+    kernel<<<blocks, threads, smem, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 
 // The library links the CUDA runtime statically, so its notion of the
 // current device is separate from the caller's: follow the device that owns
@@ -262,6 +328,7 @@ Problem<T> make_problem(void* L, void* E, void* x, const uint8_t* mask, const Di
   p.E = static_cast<T*>(E);
   p.X = static_cast<T*>(x);
   p.mask = mask;
+  p.info = nullptr;
   p.B = d.B;
   p.N = d.N;
   p.n = d.n;
@@ -334,6 +401,12 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   // Schur updates of float factors on the tcgen05 tensor cores (3xTF32), on request
   const bool upd_tc = sizeof(T) == 4 && update_tc_ok(n) && cfg.update_tensor_cores == 1;
   const size_t su_tc = (size_t)smem_update_tc_bytes(n);
+  // products of float level nodes on the tcgen05 tensor cores, on request
+  const bool node_tc = sizeof(T) == 4 && inv_first_node(n) && node_tc_ok(n, withY ? p.m : 0) &&
+                       cfg.node_tensor_cores == 1;
+  const size_t sd_tc = (size_t)smem_node_tc_bytes(n, withY ? p.m : 0);
+  auto node_tc_kernel = withY ? (inv ? k_node_tc<true, true> : k_node_tc<true, false>)
+                              : (inv ? k_node_tc<false, true> : k_node_tc<false, false>);
   long long launches = 0;
   const bool run = count == nullptr;
   const int sms = run ? sm_count() : 0;
@@ -346,6 +419,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       e = prepare(node_kernel, sd);
       if (e == cudaSuccess) e = prepare(k_update<T>, su);
       if (e == cudaSuccess && upd_tc) e = prepare(k_update_tc, su_tc);
+      if (e == cudaSuccess && node_tc) e = prepare(node_tc_kernel, sd_tc);
     }
     if (e == cudaSuccess) e = prepare(fwd_kernel, ss);
     if (e == cudaSuccess) e = prepare(pull_kernel, ss);
@@ -355,20 +429,29 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
 
   // sweep products on inverse-carrying float factors: tensor cores when the
   // launch is wider than the resident sweep CTAs (3 per SM), or as tuned
-  auto sweep_level = [&](const Level& L, long long blocks) {
+  // pre: the level's factor blocks were final before the previous kernel
+  // started (any sweep over a stored factor, and every backward level of
+  // factor_and_solve but the first), so they may be loaded before the wait
+  auto sweep_level = [&](const Level& L, long long blocks, bool pre) {
     Level o = L;
     if (cfg.sweep_tensor_cores == 1) o.tc = 1;
     else if (cfg.sweep_tensor_cores == 2) o.tc = 0;
     else o.tc = sms > 0 && blocks > 3LL * sms;
+    o.pre = pre ? 1 : 0;
     return o;
   };
+  // programmatic launches inside the op's chain on its own stream (not the
+  // first kernel, not the forked branch, not while profiling with events)
+  bool first = true;
   auto go_on = [&](cudaStream_t s, auto kernel, int kind, long long blocks, size_t smem, const Level& L,
                    int threads) {
     if (blocks <= 0) return;
     ++launches;
     if (!run) return;
+    const bool pdl = !first && s == st && g_prof == nullptr;
+    first = false;
     prof_begin(s, kind);
-    kernel<<<(unsigned)blocks, threads, smem, s>>>(p, L);
+    launch(kernel, (unsigned)blocks, (unsigned)threads, smem, s, pdl, p, L);
     prof_end(s);
   };
   auto node_threads = [&](long long blocks) {
@@ -378,15 +461,31 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   const bool forked = run && fork != nullptr && fork->ok();
 
   const bool factor = op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE;
+  if (factor && p.info != nullptr) {
+    ++launches;
+    if (run) {
+      prof_begin(st, SOCU_KIND_NODE);
+      k_info_reset<<<(p.B + 255) / 256 < 1024 ? (p.B + 255) / 256 : 1024, 256, 0, st>>>(p.info, p.B);
+      prof_end(st);
+      first = false;
+    }
+  }
   if (factor) {
     for (int l = 0; l < K; ++l) {
       const Level& L = lv[l];
       const long long node_blocks = (long long)p.B * L.d;
-      go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
+      if constexpr (sizeof(T) == 4) {
+        if (node_tc)
+          go_on(st, node_tc_kernel, SOCU_KIND_NODE, node_blocks, sd_tc, L, 256);
+        else
+          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
+      } else {
+        go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
+      }
       if (l + 1 < K) {
         // fused forward: apply this level's updates to every target vector
         const long long pull_blocks = withY ? (long long)p.B * (p.N / lv[l + 1].s) : 0;
-        const Level PL = sweep_level(lv[l + 1], pull_blocks);
+        const Level PL = sweep_level(lv[l + 1], pull_blocks, false);
         if (forked && pull_blocks > 0) {
           cudaEventRecord(fork->split, st);
           cudaStreamWaitEvent(fork->aux, fork->split, 0);
@@ -402,9 +501,10 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
         } else {
           go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L, upd_thr);
         }
-        if (forked && pull_blocks > 0)
+        if (forked && pull_blocks > 0) {
           cudaStreamWaitEvent(st, fork->join, 0);
-        else
+          first = true;   // the next node waits for the forked branch in full
+        } else
           go_on(st, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
       }
     }
@@ -412,13 +512,14 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   if (op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE) {
     for (int l = 0; l < K; ++l) {
       const long long blocks = (long long)p.B * (l == 0 ? lv[l].d : p.N / lv[l].s);
-      go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks), swp_thr);
+      go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks, true), swp_thr);
     }
   }
   if (op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE) {
     for (int l = K - 1; l >= 0; --l) {
       const long long blocks = (long long)p.B * lv[l].d;
-      go_on(st, bwd_kernel, SOCU_KIND_BACKWARD, blocks, ss, sweep_level(lv[l], blocks), swp_thr);
+      go_on(st, bwd_kernel, SOCU_KIND_BACKWARD, blocks, ss,
+            sweep_level(lv[l], blocks, op != SOCU_OP_FACTOR_AND_SOLVE || l != K - 1), swp_thr);
     }
   }
   if (count) *count = launches;
@@ -476,7 +577,8 @@ int validate(socu_op op, socu_dtype dtype, const void* L, const void* E, const v
 
 int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask,
              int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, cudaStream_t st,
-             long long* count, const Fork* fork = nullptr, const socu_tuning* over = nullptr) {
+             long long* count, const Fork* fork = nullptr, const socu_tuning* over = nullptr,
+             int32_t* info = nullptr) {
   Dims d;
   const int v = validate(op, dtype, L, E, x, batch, horizon, n, n_rhs, &d);
   if (v != SOCU_OK) return v;
@@ -494,9 +596,14 @@ int dispatch(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint
   bool inv = false;
   op = base_op(op, &inv);
   inv = inv || op == SOCU_OP_FACTOR_AND_SOLVE;
-  if (dtype == SOCU_FLOAT64)
-    return enqueue<double>(op, make_problem<double>(L, E, x, mask, d), st, count, inv, fork, over);
-  return enqueue<float>(op, make_problem<float>(L, E, x, mask, d), st, count, inv, fork, over);
+  if (dtype == SOCU_FLOAT64) {
+    Problem<double> p = make_problem<double>(L, E, x, mask, d);
+    p.info = info;
+    return enqueue<double>(op, p, st, count, inv, fork, over);
+  }
+  Problem<float> p = make_problem<float>(L, E, x, mask, d);
+  p.info = info;
+  return enqueue<float>(op, p, st, count, inv, fork, over);
 }
 
 
@@ -580,19 +687,21 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     const long long nvec = (long long)a.B * a.N * a.n * a.m;
     const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
     const int nrc = ceil_div(a.n, kResRows);
+    // each kernel follows the previous one of the round on the same stream
+    const bool pdl = g_prof == nullptr;
     prof_begin(st, SOCU_KIND_REFINE_UPDATE);
-    k_ref_update<<<upd_blocks, 256, 0, st>>>(a);
+    launch(k_ref_update, (unsigned)upd_blocks, 256, 0, st, pdl, a);
     prof_end(st);
     prof_begin(st, SOCU_KIND_RESIDUAL);
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
-                              smem_residual_x_elems(a.n) * sizeof(double), st>>>(a);
+      launch(k_residual_rows<true>, (unsigned)((long long)a.B * a.N), (unsigned)residual_rows_threads(a.n, a.m),
+             smem_residual_x_elems(a.n) * sizeof(double), st, pdl, a);
     else
-      k_residual<true><<<(unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
-                         st>>>(a);
+      launch(k_residual<true>, (unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
+             st, pdl, a);
     prof_end(st);
     prof_begin(st, SOCU_KIND_REFINE_CHECK);
-    k_ref_check<<<(a.B + 255) / 256, 256, 0, st>>>(a);
+    launch(k_ref_check, (unsigned)((a.B + 255) / 256), 256, 0, st, pdl, a);
     prof_end(st);
   } else {
     *count = 3;
@@ -839,6 +948,7 @@ struct socu_launch_s {
   double* eta = nullptr;
   int32_t* iters = nullptr;
   socu_tuning over{};               // per-launch settings (block_dim / block_size)
+  int32_t* info = nullptr;          // per-instance factor status (factor ops), may be null
 };
 
 namespace {
@@ -1076,7 +1186,7 @@ int launch_enqueue(socu_launch_s* h, cudaStream_t st, const Fork* fork = nullptr
     return refine_enqueue(h->ra, st, nullptr);
   }
   return dispatch(h->op, h->dtype, h->L, h->E, h->x, h->mask, h->batch, h->horizon, h->n, h->n_rhs, st, nullptr,
-                  fork, &h->over);
+                  fork, &h->over, h->info);
 }
 
 // Capture one run into a CUDA graph on a private stream (the legacy default
@@ -1250,6 +1360,16 @@ int socu_cholesky_run(socu_op op, socu_dtype dtype, void* L, void* E, void* x, c
   return dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, static_cast<cudaStream_t>(stream), nullptr);
 }
 
+int socu_cholesky_run_info(socu_op op, socu_dtype dtype, void* L, void* E, void* x, const uint8_t* mask,
+                           int32_t* info, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream) {
+  bool inv_op = false;
+  const socu_op bop = base_op(op, &inv_op);
+  if (info == nullptr && batch > 0) return SOCU_ERR_INVALID_ARGUMENT;
+  if (bop != SOCU_OP_FACTOR && bop != SOCU_OP_FACTOR_AND_SOLVE) return SOCU_ERR_INVALID_ARGUMENT;
+  return dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, static_cast<cudaStream_t>(stream), nullptr,
+                  nullptr, nullptr, info);
+}
+
 int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
                        const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                        int use_cuda_graph, void* stream) {
@@ -1260,11 +1380,21 @@ int socu_launch_create(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L
 int socu_launch_create_tuned(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
                              const uint8_t* mask, int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs,
                              int use_cuda_graph, const socu_tuning* settings, void* stream) {
+  return socu_launch_create_ex(out, op, dtype, L, E, x, mask, nullptr, batch, horizon, n, n_rhs, use_cuda_graph,
+                               settings, stream);
+}
+
+int socu_launch_create_ex(socu_launch_t* out, socu_op op, socu_dtype dtype, void* L, void* E, void* x,
+                          const uint8_t* mask, int32_t* info, int64_t batch, int64_t horizon, int64_t n,
+                          int64_t n_rhs, int use_cuda_graph, const socu_tuning* settings, void* stream) {
   if (out == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   if (settings && !tuning_valid(*settings)) return SOCU_ERR_INVALID_ARGUMENT;
+  bool inv_op = false;
+  const socu_op bop = base_op(op, &inv_op);
+  if (info != nullptr && bop != SOCU_OP_FACTOR && bop != SOCU_OP_FACTOR_AND_SOLVE) return SOCU_ERR_INVALID_ARGUMENT;
   long long kernels = 0;
-  int st = dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, nullptr, &kernels, nullptr, settings);
+  int st = dispatch(op, dtype, L, E, x, mask, batch, horizon, n, n_rhs, nullptr, &kernels, nullptr, settings, info);
   if (st != SOCU_OK) return st;
   socu_launch_s* h = new (std::nothrow) socu_launch_s();
   if (!h) return SOCU_ERR_UNSUPPORTED;
@@ -1282,6 +1412,7 @@ int socu_launch_create_tuned(socu_launch_t* out, socu_op op, socu_dtype dtype, v
   h->graph = nullptr;
   h->exec = nullptr;
   if (settings) h->over = *settings;
+  h->info = info;
   if (use_cuda_graph && batch > 0) {
     st = capture(h);
     if (st != SOCU_OK) {
@@ -1555,11 +1686,15 @@ int socu_launch_profile(socu_launch_t h, void* stream, double* ms, int64_t* laun
     launches[k] = 0;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  (void)cudaGetLastError();   // a stale error of an earlier, unrelated call is not this run's
   Prof prof;
   g_prof = &prof;
   int s = launch_enqueue(h, st);
   g_prof = nullptr;
   cudaError_t e = prof.err;
+  g_prof_err_kind = prof.err_kind;
+  g_prof_err_where = prof.err_where;
+  if (e != cudaSuccess) g_last_cuda_error = (int)e;
   if (s == SOCU_OK && e == cudaSuccess && !prof.stop.empty()) e = cudaEventSynchronize(prof.stop.back());
   if (s == SOCU_OK && e == cudaSuccess && prof.start.size() == prof.stop.size()) {
     for (size_t i = 0; i < prof.start.size(); ++i) {
@@ -1578,6 +1713,13 @@ int socu_launch_profile(socu_launch_t h, void* stream, double* ms, int64_t* laun
   for (cudaEvent_t ev : prof.stop) cudaEventDestroy(ev);
   if (s != SOCU_OK) return s;
   return cuda_status(e);
+}
+
+int socu_profile_error(int* kind, int* where) {
+  if (kind == nullptr || where == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  *kind = g_prof_err_kind;
+  *where = g_prof_err_where;
+  return SOCU_OK;
 }
 
 int socu_launch_destroy(socu_launch_t h) {

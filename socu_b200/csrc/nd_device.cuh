@@ -35,6 +35,7 @@ struct Problem {
   T* E;
   T* X;                  // may be null (factor only)
   const uint8_t* mask;   // may be null: all batch entries active
+  int* info;             // may be null: per batch entry, 0 or 1 + the first node whose pivot failed
   int B, N, n, m, S;
   long long sL, sE, sX;  // per-batch strides in elements
 
@@ -50,6 +51,40 @@ struct Problem {
   __device__ __forceinline__ bool active(int b) const { return mask == nullptr || mask[b] != 0; }
 };
 
+// Numerical status of one batch entry: node i failed to factor (a pivot
+// <= 0, or a non-finite value).  info keeps the failing node that comes first
+// in elimination order -- lowest level ctz(i+1), then lowest index -- so the
+// result does not depend on which node of a level reports first.  LAPACK's
+// potrf reports the failing column the same way (info > 0); the reference
+// reports nothing (socu/blas/potrf.py:97-117 takes the square root of
+// whatever pivot it meets).
+__device__ __forceinline__ void record_failure(int* info, int i) {
+  const int mine = i + 1;
+  int cur = *reinterpret_cast<volatile int*>(info);
+  while (true) {
+    if (cur != 0) {
+      const int lc = __ffs(cur) - 1, lm = __ffs(mine) - 1;
+      if (lc < lm || (lc == lm && cur <= mine)) return;
+    }
+    const int prev = atomicCAS(info, cur, mine);
+    if (prev == cur) return;
+    cur = prev;
+  }
+}
+
+// After the blocked Cholesky of node i (lower(A) = C, leading dimension lda):
+// every diagonal entry must be a positive finite number.  All threads call it.
+template <typename T>
+__device__ __forceinline__ void check_factor(const Problem<T>& p, int b, int i, const T* A, int lda) {
+  if (p.info == nullptr) return;
+  bool bad = false;
+  for (int r = threadIdx.x; r < p.n; r += blockDim.x) {
+    const T d = A[r * lda + r];
+    bad = bad || !(d > T(0)) || isinf(d);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) record_failure(p.info + b, i);
+}
+
 // One nested-dissection level (socu/block_tridiag_solver.py:869-914).
 struct Level {
   int s;    // stride 2^l
@@ -59,7 +94,17 @@ struct Level {
   int op;   // offset of the previous level's slots (unused at level 0)
   int tc;   // sweeps on inverse-carrying factors: 1 = FP64 tensor-core (DMMA) products, 0 = SIMT row dots
   int tile; // output tile of the blocked Schur update (n > 64): 16 or 32
+  int pre;  // sweeps: the factor blocks were complete before the previous kernel started, so they may be
+            // loaded before the grid-dependency wait (programmatic dependent launch)
 };
+
+// Programmatic dependent launch (sm_90+).  A kernel launched with the
+// programmatic-serialization attribute may start while its predecessor in the
+// stream is still running; pdl_wait() returns once the predecessor grid has
+// completed and its memory is visible, pdl_trigger() lets the successor start
+// launching.  Both are no-ops for kernels launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Asynchronous global -> shared copies (cp.async, element granular so that

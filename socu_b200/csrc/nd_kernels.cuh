@@ -116,6 +116,7 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
   cp_async_wait_all();
   __syncthreads();
   cta_chol_solve<T, true>(A, lda, n, V, ldv, min_i(NV, vc));
+  check_factor(p, b, i, A, lda);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
     if (c <= r) Li[e] = A[r * lda + c];
@@ -177,6 +178,7 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   cp_async_wait_all();
   __syncthreads();
   cta_chol_solve<T, true, true>(S1, ld, n, W, ld, n);   // lower(S1) = C, W = C^{-1} (zeros above)
+  check_factor(p, b, i, S1, ld);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
     Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : T(0));
@@ -208,8 +210,14 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   }
 }
 
+// info reset before a factor: 0 for every batch entry
+__global__ void k_info_reset(int* info, int B) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) info[b] = 0;
+}
+
 // node body used by the level kernels: inverse-first for small blocks
 __host__ __device__ inline bool node_uses_gemm(int n) { return n <= kNodeGemmMaxN; }
+__host__ __device__ inline bool inv_first_node(int n) { return node_uses_gemm(n); }
 // dynamic shared memory (elements) of k_node; m_y = right-hand sides solved in the node (0 without y)
 __host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int es) {
   return node_uses_gemm(n) ? smem_node_gemm_elems(n, m_y, es) : smem_node_elems(n, es);
@@ -219,6 +227,8 @@ template <typename T, bool WITH_Y, bool INV = false>
 __global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
+  pdl_wait();
+  pdl_trigger();
   if (!p.active(b)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (node_uses_gemm(p.n))
@@ -381,6 +391,8 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
   const int per_b = update_launch_tasks(p.n, p.N, lv);
   const int b = blockIdx.x / per_b;
   const int task = blockIdx.x - b * per_b;
+  pdl_wait();
+  pdl_trigger();
   if (!p.active(b)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (update_uses_full(p.n))
@@ -837,11 +849,14 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
   T* dv = RES ? Gs + n * ldm : Ms + n * (kTile + 1);
   T* yj = p.Xb(b, j);
   const T* Lj = p.Lb(b, j);
+  if (!lv.pre) pdl_wait();
   if (RES) {
     if (solve) async_load(Cs, ldm, Lj, n, n, n);
     if (F) async_load(Fs, ldm, F, n, n, n);
     if (G) async_load(Gs, ldm, G, n, n, n);
   }
+  if (lv.pre) pdl_wait();
+  pdl_trigger();
   for (int c0 = 0; c0 < p.m; c0 += kMC) {
     const int mc = min_i(kMC, p.m - c0);
     __syncthreads();
@@ -918,11 +933,14 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
   const T* G = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
   const T* Li = p.Lb(b, i);
   T* xi = p.Xb(b, i);
+  if (!lv.pre) pdl_wait();
   if (RES) {
     async_load(Cs, ldm, Li, n, n, n);
     if (right) async_load(Fs, ldm, F, n, n, n);
     if (left) async_load(Gs, ldm, G, n, n, n);
   }
+  if (lv.pre) pdl_wait();
+  pdl_trigger();
   for (int c0 = 0; c0 < p.m; c0 += kMC) {
     const int mc = min_i(kMC, p.m - c0);
     __syncthreads();

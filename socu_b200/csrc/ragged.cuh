@@ -84,6 +84,7 @@ __host__ __device__ inline Level rg_level(int N, int l) {
   lv.op = prev;
   lv.tc = 0;       // persistent CTAs: SIMT sweep products (lower latency per node)
   lv.tile = 32;    // unused (n <= 64: whole-block updates)
+  lv.pre = 0;      // no programmatic launches in the persistent kernel
   return lv;
 }
 
@@ -248,6 +249,7 @@ __device__ __forceinline__ Problem<T> rg_problem(const RgArgs<T>& a, const RgIns
   p.E = a.E + I.oE;
   p.X = a.X + I.oX;
   p.mask = nullptr;
+  p.info = nullptr;
   p.B = 1;
   p.N = I.N;
   p.n = I.n;

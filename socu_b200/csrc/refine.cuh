@@ -61,6 +61,8 @@ __device__ __forceinline__ double block_max(double v, double* red) {
 
 // Per-instance state reset (before k_ref_init accumulates into it).
 __global__ void k_ref_reset(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
     const bool on = a.mask == nullptr || a.mask[bi] != 0;
     a.active[bi] = on ? 1 : 0;
@@ -126,6 +128,8 @@ __device__ __forceinline__ void ref_init_body(const RefineArgs& a, int bi, int i
 }
 
 __global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int per = a.N > a.S ? a.N : a.S;
   const int bi = blockIdx.x / per;
   const int i = blockIdx.x - bi * per;
@@ -135,6 +139,8 @@ __global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
 
 // x += delta (R32) for active instances; grid-stride over the whole batch.
 __global__ void __launch_bounds__(256) k_ref_update(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const long long per = (long long)a.N * a.n * a.m;
   const long long total = (long long)a.B * per;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
@@ -223,6 +229,8 @@ __device__ __forceinline__ void residual_body(const RefineArgs& a, int bi, int i
 
 template <bool REFINE>
 __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int nrc = (a.n + kResRows - 1) / kResRows;
   const int per = a.N * nrc;
   const int bi = blockIdx.x / per;
@@ -347,6 +355,8 @@ __host__ __device__ inline int residual_rows_threads(int n, int) { return 32 * (
 
 template <bool REFINE>
 __global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int bi = blockIdx.x / a.N;
   const int i = blockIdx.x - bi * a.N;
   if (REFINE && !a.active[bi]) return;
@@ -443,6 +453,8 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
 }
 
 __global__ void __launch_bounds__(256) k_ref_init_rows(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int per = a.N > a.S ? a.N : a.S;
   const int bi = blockIdx.x / per;
   const int i = blockIdx.x - bi * per;
@@ -455,6 +467,8 @@ __global__ void __launch_bounds__(256) k_ref_init_rows(RefineArgs a) {
 // A non-finite eta (numerical breakdown of the float factor) stops the
 // instance with iters = -(iterations done).
 __global__ void k_ref_check(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
   for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
     if (!a.active[bi]) continue;
     RefineState& s = a.st[bi];

@@ -154,12 +154,12 @@ __device__ __forceinline__ void put_split(unsigned char* hi, unsigned char* lo, 
   *reinterpret_cast<float*>(lo + o) = v - h;
 }
 
-// One thread: the 3xTF32 MMAs of D (128 x N) (+)= A * B^T over K (multiple of
-// 8), operand planes at shared addresses a_hi, a_lo (128 rows x K) and b_hi,
+// One thread: the 3xTF32 MMAs of D (M x N) (+)= A * B^T over K (multiple of
+// 8), operand planes at shared addresses a_hi, a_lo (M rows x K) and b_hi,
 // b_lo (N rows x K) in the layout above; accumulate = 0 overwrites D first.
 __device__ __forceinline__ void gemm_3xtf32(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
-                                            uint32_t b_lo, int N, int K, uint32_t accumulate) {
-  const uint32_t idesc = idesc_tf32(128, N);
+                                            uint32_t b_lo, int N, int K, uint32_t accumulate, int M = 128) {
+  const uint32_t idesc = idesc_tf32(M, N);
   const uint32_t sbo = (uint32_t)(K >> 2) * 128u;
   for (int s = 0; s < K / 8; ++s) {
     const uint32_t off = (uint32_t)s * 256u;

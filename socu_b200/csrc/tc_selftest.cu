@@ -1,9 +1,11 @@
 // Self-test of the tcgen05 building block (tc_gemm.cuh): one CTA computes
-// D (128 x N) = A (128 x K) * B (N x K)^T with the 3xTF32 split, FP32
-// accumulation in tensor memory, through exactly the staging, descriptor,
-// MMA, commit and TMEM-load path the solver kernels use.  Exposed through the
-// C ABI so that the path can be checked against a host reference in
-// isolation.
+// D (M x N) = A (M x K) * B (N x K)^T, M = 64 or 128, with the 3xTF32 split,
+// FP32 accumulation in tensor memory, through exactly the staging,
+// descriptor, MMA, commit and TMEM-load path the solver kernels use, and
+// writes all 128 TMEM lanes of the accumulator's N columns to D (lane-major),
+// so that the row-to-lane placement of an M = 64 accumulator can be checked
+// too.  Exposed through the C ABI so that the path can be checked against a
+// host reference in isolation.
 #include <cuda_runtime.h>
 
 #include "../../include/socu_b200.h"
@@ -16,7 +18,7 @@ using namespace socu;
 constexpr unsigned long long kTcWaitNs = 200000000ull;   // 0.2 s bound of every tensor-core wait
 
 __global__ void __launch_bounds__(256, 1) k_tc_selftest(const float* __restrict__ A, const float* __restrict__ B,
-                                                         float* __restrict__ D, int N, int K, int* err) {
+                                                         float* __restrict__ D, int M, int N, int K, int* err) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tbase;
@@ -28,7 +30,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_selftest(const float* __restrict_
   unsigned char* b_lo = b_hi + N * K * 4;
   if (warp == 0) tc::tmem_alloc(&tbase, ncols);
   if (tid == 0) tc::mbar_init(&bar, 1);
-  for (int e = tid; e < 128 * K; e += blockDim.x) tc::put_split(a_hi, a_lo, e / K, e % K, K, A[e]);
+  for (int e = tid; e < 128 * K; e += blockDim.x)
+    tc::put_split(a_hi, a_lo, e / K, e % K, K, e / K < M ? A[e] : 0.0f);
   for (int e = tid; e < N * K; e += blockDim.x) tc::put_split(b_hi, b_lo, e / K, e % K, K, B[e]);
   tc::fence_async_smem();
   tc::fence_before_sync();
@@ -36,7 +39,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_selftest(const float* __restrict_
   tc::fence_after_sync();
   const uint32_t d = tbase;
   if (tid == 0) {
-    tc::gemm_3xtf32(d, tc::saddr(a_hi), tc::saddr(a_lo), tc::saddr(b_hi), tc::saddr(b_lo), N, K, 0u);
+    tc::gemm_3xtf32(d, tc::saddr(a_hi), tc::saddr(a_lo), tc::saddr(b_hi), tc::saddr(b_lo), N, K, 0u, M);
     tc::commit(&bar);
   }
   bool ok = tc::mbar_wait(&bar, 0, kTcWaitNs);
@@ -63,9 +66,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_selftest(const float* __restrict_
 
 }  // namespace
 
-extern "C" int socu_tc_selftest(const float* A, const float* B, float* D, int64_t n_cols, int64_t k_depth,
-                                int* error_flag, void* stream) {
+extern "C" int socu_tc_selftest(const float* A, const float* B, float* D, int64_t m_rows, int64_t n_cols,
+                                int64_t k_depth, int* error_flag, void* stream) {
   if (A == nullptr || B == nullptr || D == nullptr || error_flag == nullptr) return SOCU_ERR_INVALID_ARGUMENT;
+  if (m_rows != 64 && m_rows != 128) return SOCU_ERR_INVALID_ARGUMENT;
   if (n_cols < 16 || n_cols > 128 || n_cols % 16 != 0 || k_depth < 8 || k_depth % 8 != 0)
     return SOCU_ERR_INVALID_ARGUMENT;
   const size_t smem = (size_t)(128 + n_cols) * (size_t)k_depth * 4 * 2;
@@ -76,7 +80,7 @@ extern "C" int socu_tc_selftest(const float* A, const float* B, float* D, int64_
   if (smem + 1024 > (size_t)optin) return SOCU_ERR_UNSUPPORTED;
   if (cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return SOCU_ERR_CUDA;
-  k_tc_selftest<<<1, 256, smem, static_cast<cudaStream_t>(stream)>>>(A, B, D, (int)n_cols, (int)k_depth,
-                                                                      error_flag);
+  k_tc_selftest<<<1, 256, smem, static_cast<cudaStream_t>(stream)>>>(A, B, D, (int)m_rows, (int)n_cols,
+                                                                      (int)k_depth, error_flag);
   return cudaGetLastError() == cudaSuccess ? SOCU_OK : SOCU_ERR_CUDA;
 }

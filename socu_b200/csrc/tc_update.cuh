@@ -156,12 +156,160 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(Problem<float> p, Level lv
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
+  pdl_wait();
+  pdl_trigger();
   unsigned phase = 0;
   update_tc_body(p, lv, b, task, smem_raw, tbase, &bar, &phase);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   if (warp == 0) tc::tmem_dealloc(tbase, 128);
+}
+
+// ---------------------------------------------------------------------------
+// Level node of a FLOAT factor (n <= 64) with its products on the tcgen05
+// tensor cores.  The factor part is the inverse-first node's (node_gemm_body:
+// blocked Cholesky of L_i against the identity, C W = I, W = C^{-1}); the
+// three products that follow -- F = R W^T (right slot), G = W Lf (left slot),
+// y = W y (factor_and_solve) -- share the operand W and run as one MMA group
+//     D (n x NB) = W * Bm^T,   Bm rows: the n rows of R, the n columns of Lf,
+//                              the m columns of y  (NB = nr + nl + m <= 256)
+// so D's first n columns hold F^T, the next n G and the last m W y.
+// socu: trsm_rltn / trsm_llnn (K3/K4) and the fused forward step,
+// socu/block_tridiag_solver.py:219-279, :108-110, done here as products with
+// the explicit inverse.  The MMA has M = 64 rows (rows n..63 of W are zero):
+// row r of D sits in TMEM lane 32 (r / 16) + r % 16.
+// ---------------------------------------------------------------------------
+constexpr int kTcNodeMaxN = 64;
+constexpr int kTcNodeMaxCols = 256;
+__host__ __device__ inline int tc_node_cols(int n, bool right, bool left, int m) {
+  return tc_ncols((right ? n : 0) + (left ? n : 0) + m);
+}
+__host__ __device__ inline uint32_t tmem_cols_for(int cols) {
+  return cols <= 32 ? 32u : (cols <= 64 ? 64u : (cols <= 128 ? 128u : 256u));
+}
+// shared memory: S1, W (n x gemm_ld) for the factor, then the A (64 rows) and
+// B (up to kTcNodeMaxCols rows) hi/lo planes of one K chunk
+__host__ __device__ inline long long smem_node_tc_bytes(int n, int m) {
+  const long long simt = 2LL * n * gemm_ld(n, 4) * 4;
+  return ((simt + 127) / 128) * 128 + 2LL * 64 * kTcKC * 4 + 2LL * tc_ncols(2 * n + m) * kTcKC * 4;
+}
+__host__ __device__ inline bool node_tc_ok(int n, int m) {
+  return n >= 1 && n <= kTcNodeMaxN && tc_ncols(2 * n + m) <= kTcNodeMaxCols;
+}
+
+template <bool WITH_Y, bool INV>
+__device__ __forceinline__ void node_tc_body(const Problem<float>& p, const Level& lv, int b, int t,
+                                             unsigned char* smem, uint32_t tmem, uint64_t* bar, unsigned* phase) {
+  const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
+  const bool right = i + s < p.N, left = t >= 1;
+  const int ld = gemm_ld(n, 4);
+  float* S1 = reinterpret_cast<float*>(smem);
+  float* W = S1 + n * ld;
+  const long long simt = 2LL * n * ld * 4;
+  unsigned char* a_hi = smem + ((simt + 127) / 128) * 128;
+  unsigned char* a_lo = a_hi + 64 * kTcKC * 4;
+  unsigned char* b_hi = a_lo + 64 * kTcKC * 4;
+  const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0;
+  const int NB = nr + nl + ny, NBp = tc_ncols(NB);
+  unsigned char* b_lo = b_hi + NBp * kTcKC * 4;
+  float* Li = p.Lb(b, i);
+  float* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
+  float* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
+  float* yi = WITH_Y ? p.Xb(b, i) : nullptr;
+  const int m = p.m;
+
+  // factor: lower(S1) = C, W = C^{-1}
+  async_load(S1, ld, Li, n, n, n);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - r * n;
+    W[r * ld + c] = r == c ? 1.0f : 0.0f;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  cta_chol_solve<float, true, true>(S1, ld, n, W, ld, n);
+  check_factor(p, b, i, S1, ld);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - r * n;
+    Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : 0.0f);
+  }
+  if (NB == 0) return;
+  // products on the tensor cores, K = n in chunks of kTcKC
+  for (int k0 = 0; k0 < n; k0 += kTcKC) {
+    tc_stage(a_hi, a_lo, 64, n, n, k0, [&](int r, int k) { return W[r * ld + k]; });
+    tc_stage(b_hi, b_lo, NBp, NB, n, k0, [&](int c, int k) {
+      if (c < nr) return R[(long long)c * n + k];
+      if (c < nr + nl) return Lf[(long long)k * n + (c - nr)];
+      return yi[(long long)k * m + (c - nr - nl)];
+    });
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0) {
+      tc::gemm_3xtf32(tmem, tc::saddr(a_hi), tc::saddr(a_lo), tc::saddr(b_hi), tc::saddr(b_lo), NBp, kTcKC,
+                      k0 > 0 ? 1u : 0u, 64);
+      tc::commit(bar);
+    }
+    const bool done = tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+    const bool ok = __syncthreads_and(done) != 0;
+    tc::fence_after_sync();
+    if (!ok) {
+      tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+      if (threadIdx.x == 0) atomicExch(&g_tc_error, 1);
+      *phase += 1;
+      return;
+    }
+    *phase += 1;
+  }
+  // epilogue: warp w reads rows 16 (w % 4) .. +15 (lanes 0-15 of its
+  // sub-partition), columns split between the blockDim / 128 warps of a quadrant
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3, parts = blockDim.x / 128, h = warp >> 2;
+  const int r = 16 * q + lane;
+  const int span = ((NBp / 8 + parts - 1) / parts) * 8;
+  const int c_begin = h * span, c_end = min_i(NB, c_begin + span);
+  if (16 * q >= n) return;
+  for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+    float v[8];
+    tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+    tc::tmem_wait_ld();
+    if (lane < 16 && r < n) {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int c = c0 + e;
+        if (c < nr) R[(long long)c * n + r] = v[e];                  // F[c][r] = D[r][c]
+        else if (c < nr + nl) Lf[(long long)r * n + (c - nr)] = v[e];  // G[r][c - nr]
+        else if (c < NB) yi[(long long)r * m + (c - nr - nl)] = v[e];
+      }
+    }
+  }
+}
+
+template <bool WITH_Y, bool INV>
+__global__ void __launch_bounds__(256, 1) k_node_tc(Problem<float> p, Level lv) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  const int b = blockIdx.x / lv.d;
+  const int t = blockIdx.x - b * lv.d;
+  if (!p.active(b)) return;
+  const int i = lv.s - 1 + 2 * lv.s * t;
+  const uint32_t ncols = tmem_cols_for(tc_node_cols(p.n, i + lv.s < p.N, t >= 1, WITH_Y ? p.m : 0));
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) tc::tmem_alloc(&tbase, ncols);
+  if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  pdl_wait();
+  pdl_trigger();
+  unsigned phase = 0;
+  node_tc_body<WITH_Y, INV>(p, lv, b, t, smem_raw, tbase, &bar, &phase);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tbase, ncols);
 }
 
 }  // namespace socu
