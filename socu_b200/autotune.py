@@ -16,6 +16,8 @@ Settings (``socu_tuning``; 0 = built-in heuristic):
     ragged_units         level nodes per task chunk of a ragged batch: 1..64
     update_tensor_cores  Schur updates of float factors (n <= 128) on the
                          tcgen05 tensor cores, 3xTF32 (1), or not (2)
+    node_tensor_cores    products of float level nodes (n <= 64) on the
+                         tcgen05 tensor cores (1) or SIMT (2)
 
 Search: coordinate descent from the built-in heuristics.  Each knob in turn
 is tried at every value with the others held at the best so far; a candidate
@@ -47,8 +49,8 @@ from . import _lib
 __all__ = ["cache_path", "load_cache", "save_entry", "tune", "candidates", "current_settings", "install",
            "KNOBS", "maybe_autotune"]
 
-KNOBS = ("update_tensor_cores", "node_threads", "sweep_tensor_cores", "sweep_threads", "update_threads",
-         "update_tile")
+KNOBS = ("update_tensor_cores", "node_tensor_cores", "node_threads", "sweep_tensor_cores", "sweep_threads",
+         "update_threads", "update_tile")
 _VALUES = {
     "node_threads": (0, 64, 128, 256),
     "update_threads": (0, 128, 256),
@@ -56,6 +58,7 @@ _VALUES = {
     "sweep_tensor_cores": (0, 1, 2),
     "update_tile": (0, 16, 32),
     "update_tensor_cores": (0, 1, 2),
+    "node_tensor_cores": (0, 1, 2),
 }
 _loaded = set()
 _tuned = set()
@@ -158,6 +161,8 @@ def candidates(n: int, n_rhs: int, dtype) -> dict:
         if k == "sweep_tensor_cores" and (n > 64 or _dtype_name(dtype) == "float64"):
             continue
         if k == "update_tensor_cores" and (n > 128 or _dtype_name(dtype) == "float64"):
+            continue
+        if k == "node_tensor_cores" and (n > 64 or 2 * n + n_rhs > 256 or _dtype_name(dtype) == "float64"):
             continue
         out[k] = vals
     return out

@@ -25,7 +25,7 @@ def test_table_exact_and_wildcard_entries():
     # exact entry on top of the wildcard one
     assert autotune.current_settings(torch.float32, 64, 8) == {
         "node_threads": 128, "update_threads": 0, "sweep_threads": 256, "sweep_tensor_cores": 2,
-        "update_tile": 0, "ragged_units": 0, "update_tensor_cores": 0}
+        "update_tile": 0, "ragged_units": 0, "update_tensor_cores": 0, "node_tensor_cores": 0}
     # other n_rhs: wildcard only
     assert autotune.current_settings(torch.float32, 64, 3)["node_threads"] == 128
     assert autotune.current_settings(torch.float32, 64, 3)["sweep_threads"] == 0
@@ -40,7 +40,8 @@ def test_table_exact_and_wildcard_entries():
 
 
 @pytest.mark.parametrize("bad", [{"node_threads": 96}, {"update_tile": 8}, {"sweep_tensor_cores": 3},
-                                 {"ragged_units": 65}, {"sweep_threads": 512}, {"update_tensor_cores": 3}])
+                                 {"ragged_units": 65}, {"sweep_threads": 512}, {"update_tensor_cores": 3},
+                                 {"node_tensor_cores": -1}])
 def test_table_rejects_invalid_settings(bad):
     with pytest.raises(RuntimeError):
         autotune.install(torch.float64, 16, 1, bad)
