@@ -376,6 +376,25 @@ def run_ours(args, rank, world, local_rank):
     del prof_mixed
     dmma_tf = dmma_peak_tflops(dev)
 
+    # the other shifts of this configuration: s = 1 and 0.1 make the README
+    # matrix numerically indefinite (the diagonal factor blocks tril(randn) + s I
+    # are numerically singular), so both paths must report the breakdown
+    shift_sweep = {f"{SHIFT:g}": {"mixed_eta": eta_dev, "mixed_iterations": iters, "fp64_info": 0}}
+    for s_alt in (1.0, 0.1):
+        from socu_b200.problems import readme_blocks
+        La, Ea, ba = readme_blocks(N_BLOCKS, BLOCK, NRHS, shift=s_alt, seed=SEED, batch=1, device=dev)
+        xa = torch.zeros_like(ba)
+        ra = create_cholesky_refined_solve_launch(La, Ea, ba, xa, tol=TOL, max_iter=3, use_cuda_graph=False)
+        ra()
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+        create_cholesky_factor_and_solve_launch(La, Ea, ba, info=info)()
+        torch.cuda.synchronize(dev)
+        shift_sweep[f"{s_alt:g}"] = {"mixed_eta": float(ra.eta.max()), "mixed_iterations": int(ra.iterations.min()),
+                                     "fp64_info": int(info[0]),
+                                     "status": "breakdown reported (numerically indefinite)"
+                                     if (int(info[0]) != 0 and not float(ra.eta.max()) <= TOL) else "solved"}
+        del La, Ea, ba, xa, ra
+
     # e2e through the public API with host buffers (pinned), copies inside the timed region
     Lh = L0.cpu().pin_memory(); Eh = E0.cpu().pin_memory(); bh = b0.cpu().pin_memory()
     xh = torch.empty_like(x, device="cpu").pin_memory()
@@ -501,6 +520,7 @@ def run_ours(args, rank, world, local_rank):
                        "phases": budget(phases_plain)},
         "mixed_over_fp64": sec_plain / sec_mixed,
         "backward_error": {"max": eta_dev, "recomputed": eta_check, "iterations": iters},
+        "shift_sweep": dict(shift_sweep, note="fp64_info: 1 + first failing node of the plain FP64 factor, 0 = SPD"),
         "forward_error": {"mixed": fwd_mixed, "fp64_plain": fwd_plain,
                           "reference": "LAPACK banded FP64 Cholesky (scipy solveh_banded) of the same system"},
         "factor_flops_fp": fac_flops,

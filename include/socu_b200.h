@@ -140,9 +140,11 @@ int socu_launch_run(socu_launch_t launch, void* stream);
  * blocked Schur update for n > 64 (16 or 32; the reference's block_size).
  * ragged_units: level nodes per task chunk of a ragged batch (1..64).
  * update_tensor_cores: Schur updates of float factors (n <= 128) on the
- * tcgen05 tensor cores with 3xTF32 operands (1) or on the FP64 / SIMT path (2).
+ * tcgen05 tensor cores with 3xTF32 operands (1) or on the FP64 tensor pipe
+ * (2, the default: exact products of the float operands, FP64 sums).
  * node_tensor_cores: the coupling and forward products of float level nodes
- * (n <= 64, 2n + n_rhs <= 256) on the tcgen05 tensor cores (1) or SIMT (2). */
+ * (n <= 128) on the tcgen05 tensor cores at every level (1), only on levels
+ * with at least 4 nodes per SM (3), or SIMT (2, and the default). */
 typedef struct socu_tuning {
   int32_t node_threads;
   int32_t update_threads;
@@ -202,9 +204,10 @@ typedef enum socu_kernel_kind {
  * events add gaps between kernels. */
 int socu_launch_profile(socu_launch_t launch, void* stream, double* ms, int64_t* launches);
 
-/* After a failed socu_launch_profile in this thread: the kernel kind of the
- * launch the error was charged to (-1 if none) and whether the error was
- * already pending before that launch (0) or raised by it (1). */
+/* After a failed socu_launch_profile in this thread: the kernel kind the
+ * error was charged to (-1 if none) and where it arose: 0 pending before that
+ * launch, 1 raised by the launch, 2 creating or recording a timing event, 3 a
+ * non-launch call of the op, 4 synchronising on or reading the events. */
 int socu_profile_error(int* kind, int* where);
 
 /* Number of kernels one run enqueues (0 for a NULL launch).  For a

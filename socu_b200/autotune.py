@@ -16,8 +16,9 @@ Settings (``socu_tuning``; 0 = built-in heuristic):
     ragged_units         level nodes per task chunk of a ragged batch: 1..64
     update_tensor_cores  Schur updates of float factors (n <= 128) on the
                          tcgen05 tensor cores, 3xTF32 (1), or not (2)
-    node_tensor_cores    products of float level nodes (n <= 64) on the
-                         tcgen05 tensor cores (1) or SIMT (2)
+    node_tensor_cores    products of float level nodes (n <= 128) on the
+                         tcgen05 tensor cores at every level (1), on wide
+                         levels only (3), or SIMT (2)
 
 Search: coordinate descent from the built-in heuristics.  Each knob in turn
 is tried at every value with the others held at the best so far; a candidate
@@ -58,7 +59,7 @@ _VALUES = {
     "sweep_tensor_cores": (0, 1, 2),
     "update_tile": (0, 16, 32),
     "update_tensor_cores": (0, 1, 2),
-    "node_tensor_cores": (0, 1, 2),
+    "node_tensor_cores": (0, 1, 3),
 }
 _loaded = set()
 _tuned = set()
@@ -162,7 +163,7 @@ def candidates(n: int, n_rhs: int, dtype) -> dict:
             continue
         if k == "update_tensor_cores" and (n > 128 or _dtype_name(dtype) == "float64"):
             continue
-        if k == "node_tensor_cores" and (n > 64 or 2 * n + n_rhs > 256 or _dtype_name(dtype) == "float64"):
+        if k == "node_tensor_cores" and (n > 128 or _dtype_name(dtype) == "float64"):
             continue
         out[k] = vals
     return out

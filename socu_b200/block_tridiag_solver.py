@@ -201,8 +201,9 @@ def _profiler(lib, h, sh, dev):
             kind, where = ctypes.c_int(-1), ctypes.c_int(-1)
             lib.socu_profile_error(ctypes.byref(kind), ctypes.byref(where))
             name = _lib.KIND_NAMES[kind.value] if 0 <= kind.value < _lib.KIND_COUNT else "none"
-            _lib.check(status, f"socu_launch_profile (at a {name} launch, "
-                               f"{'raised by it' if where.value == 1 else 'pending before it'})")
+            places = {0: "pending before a launch", 1: "raised by a launch", 2: "recording a timing event",
+                      3: "in a non-launch call of the op", 4: "reading the timing events"}
+            _lib.check(status, f"socu_launch_profile ({places.get(where.value, 'unknown')}, kernel kind {name})")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES) if cnt[i]}
     return profile
 

@@ -183,7 +183,7 @@ bool tuning_valid(const socu_tuning& t) {
   return thr(t.node_threads) && thr(t.update_threads) && thr(t.sweep_threads) && t.sweep_tensor_cores >= 0 &&
          t.sweep_tensor_cores <= 2 && (t.update_tile == 0 || t.update_tile == 16 || t.update_tile == 32) &&
          t.ragged_units >= 0 && t.ragged_units <= 64 && t.update_tensor_cores >= 0 && t.update_tensor_cores <= 2 &&
-         t.node_tensor_cores >= 0 && t.node_tensor_cores <= 2;
+         t.node_tensor_cores >= 0 && t.node_tensor_cores <= 3;
 }
 
 void tuning_merge(socu_tuning* into, const socu_tuning& over) {
@@ -221,7 +221,8 @@ struct Prof {
   std::vector<int> kind;
   cudaError_t err = cudaSuccess;
   int err_kind = -1;    // kernel kind of the first failing launch
-  int err_where = -1;   // 0: error pending before that launch, 1: raised by it
+  int err_where = -1;   // 0: error pending before that launch, 1: raised by it, 2: event create / record,
+                        // 3: a non-launch call of the op, 4: event synchronise / elapsed time
 };
 // kind and place of the last profiling failure in this thread (socu_profile_error)
 thread_local int g_prof_err_kind = -1, g_prof_err_where = -1;
@@ -233,7 +234,11 @@ void prof_mark(cudaStream_t s, bool begin, int kind) {
   cudaError_t r = cudaEventCreate(&e);
   if (r == cudaSuccess) r = cudaEventRecord(e, s);
   if (r != cudaSuccess) {
-    if (g_prof->err == cudaSuccess) g_prof->err = r;
+    if (g_prof->err == cudaSuccess) {
+      g_prof->err = r;
+      g_prof->err_kind = kind;
+      g_prof->err_where = 2;   // event create / record
+    }
     if (e) cudaEventDestroy(e);
     return;
   }
@@ -398,12 +403,20 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   auto fwd_kernel = res ? (inv ? k_fwd<T, true, false, true> : k_fwd<T, true>) : k_fwd<T, false>;
   auto pull_kernel = res ? k_fwd<T, true, true> : k_fwd<T, false, true>;
   auto bwd_kernel = res ? (inv ? k_bwd<T, true, true> : k_bwd<T, true>) : k_bwd<T, false>;
-  // Schur updates of float factors on the tcgen05 tensor cores (3xTF32), on request
+  // Schur updates of float factors on the tcgen05 tensor cores (3xTF32), on
+  // request: the FP64-pipe updates (exact products of the float operands,
+  // FP64 sums) keep the float factor accurate enough for the reference's
+  // float tolerances and for three refinement rounds instead of five
   const bool upd_tc = sizeof(T) == 4 && update_tc_ok(n) && cfg.update_tensor_cores == 1;
   const size_t su_tc = (size_t)smem_update_tc_bytes(n);
-  // products of float level nodes on the tcgen05 tensor cores, on request
-  const bool node_tc = sizeof(T) == 4 && inv_first_node(n) && node_tc_ok(n, withY ? p.m : 0) &&
-                       cfg.node_tensor_cores == 1;
+  // products of float level nodes on the tcgen05 tensor cores: on request
+  // (node_tensor_cores = 1) at every level, or with node_tensor_cores = 3 only
+  // on levels wide enough to be throughput-bound (at least 4 nodes per SM),
+  // where the SIMT products cost more issue slots than the MMA round trips
+  const bool node_tc_any = sizeof(T) == 4 && node_tc_ok(n, withY ? p.m : 0) &&
+                           (cfg.node_tensor_cores == 1 || cfg.node_tensor_cores == 3) &&
+                           (long long)smem_node_tc_bytes(n, withY ? p.m : 0) <= (long long)max_smem_optin();
+  const bool node_tc_wide_only = cfg.node_tensor_cores == 3;
   const size_t sd_tc = (size_t)smem_node_tc_bytes(n, withY ? p.m : 0);
   auto node_tc_kernel = withY ? (inv ? k_node_tc<true, true> : k_node_tc<true, false>)
                               : (inv ? k_node_tc<false, true> : k_node_tc<false, false>);
@@ -417,9 +430,9 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     cudaError_t e = cudaSuccess;
     if (op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE) {
       e = prepare(node_kernel, sd);
-      if (e == cudaSuccess) e = prepare(k_update<T>, su);
+      if (e == cudaSuccess) e = update_uses_big(n) ? prepare(k_update_big<T>, su) : prepare(k_update<T>, su);
       if (e == cudaSuccess && upd_tc) e = prepare(k_update_tc, su_tc);
-      if (e == cudaSuccess && node_tc) e = prepare(node_tc_kernel, sd_tc);
+      if (e == cudaSuccess && node_tc_any) e = prepare(node_tc_kernel, sd_tc);
     }
     if (e == cudaSuccess) e = prepare(fwd_kernel, ss);
     if (e == cudaSuccess) e = prepare(pull_kernel, ss);
@@ -475,6 +488,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       const Level& L = lv[l];
       const long long node_blocks = (long long)p.B * L.d;
       if constexpr (sizeof(T) == 4) {
+        const bool node_tc = node_tc_any && (!node_tc_wide_only || node_blocks >= 4LL * sms);
         if (node_tc)
           go_on(st, node_tc_kernel, SOCU_KIND_NODE, node_blocks, sd_tc, L, 256);
         else
@@ -492,14 +506,19 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
           go_on(fork->aux, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
           cudaEventRecord(fork->join, fork->aux);
         }
+        const long long upd_blocks = (long long)p.B * update_launch_tasks(n, p.N, L);
+        bool tc_done = false;
         if constexpr (sizeof(T) == 4) {
-          if (upd_tc)
+          if (upd_tc) {
             go_on(st, k_update_tc, SOCU_KIND_UPDATE, (long long)p.B * update_blocks(p.N, L), su_tc, L, 256);
+            tc_done = true;
+          }
+        }
+        if (!tc_done) {
+          if (update_uses_big(n))
+            go_on(st, k_update_big<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, 256);
           else
-            go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L,
-                  upd_thr);
-        } else {
-          go_on(st, k_update<T>, SOCU_KIND_UPDATE, (long long)p.B * update_launch_tasks(n, p.N, L), su, L, upd_thr);
+            go_on(st, k_update<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, upd_thr);
         }
         if (forked && pull_blocks > 0) {
           cudaStreamWaitEvent(st, fork->join, 0);
@@ -1692,16 +1711,20 @@ int socu_launch_profile(socu_launch_t h, void* stream, double* ms, int64_t* laun
   int s = launch_enqueue(h, st);
   g_prof = nullptr;
   cudaError_t e = prof.err;
-  g_prof_err_kind = prof.err_kind;
-  g_prof_err_where = prof.err_where;
+  if (s != SOCU_OK && e == cudaSuccess) prof.err_where = 3;
   if (e != cudaSuccess) g_last_cuda_error = (int)e;
-  if (s == SOCU_OK && e == cudaSuccess && !prof.stop.empty()) e = cudaEventSynchronize(prof.stop.back());
+  if (s == SOCU_OK && e == cudaSuccess && !prof.stop.empty()) {
+    e = cudaEventSynchronize(prof.stop.back());
+    if (e != cudaSuccess) prof.err_where = 4;
+  }
   if (s == SOCU_OK && e == cudaSuccess && prof.start.size() == prof.stop.size()) {
     for (size_t i = 0; i < prof.start.size(); ++i) {
       float t = 0.f;
       const cudaError_t r = cudaEventElapsedTime(&t, prof.start[i], prof.stop[i]);
       if (r != cudaSuccess) {
         e = r;
+        prof.err_where = 4;
+        prof.err_kind = prof.kind[i];
         break;
       }
       const int k = prof.kind[i] >= 0 && prof.kind[i] < SOCU_KIND_COUNT ? prof.kind[i] : SOCU_KIND_COUNT - 1;
@@ -1711,6 +1734,8 @@ int socu_launch_profile(socu_launch_t h, void* stream, double* ms, int64_t* laun
   }
   for (cudaEvent_t ev : prof.start) cudaEventDestroy(ev);
   for (cudaEvent_t ev : prof.stop) cudaEventDestroy(ev);
+  g_prof_err_kind = prof.err_kind;
+  g_prof_err_where = prof.err_where;
   if (s != SOCU_OK) return s;
   return cuda_status(e);
 }

@@ -37,9 +37,12 @@ __host__ __device__ inline int min_i(int a, int b) { return a < b ? a : b; }
 // shared-memory sizes (elements) ------------------------------------------------
 __host__ __device__ inline int gemm_ld(int n, int es) { return es == 8 ? ((n + 15) / 16) * 16 + 4 : n + 1; }
 // vectors solved per pass of k_node (items beyond the block size loop)
-__host__ __device__ inline int node_chunk(int n) { return n <= 64 ? 232 : 64; }
+// (n > 64: as many as fit beside the n x n block in 227 KB -- all 2n + 32 of
+// a 128-block node with 32 right-hand sides in one pass for float, 80 per pass
+// for double)
+__host__ __device__ inline int node_chunk(int n, int es) { return n <= 64 ? 232 : (es == 4 ? 304 : 80); }
 __host__ __device__ inline long long smem_node_elems(int n, int es) {
-  return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n), es);
+  return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n, es), es);
 }
 __host__ __device__ inline int update_ld(int k, int es) { return gemm_ld(k, es); }
 // blocked Schur update (n > 64) with tile x tile output tiles
@@ -48,16 +51,22 @@ __host__ __device__ inline long long smem_update_elems(int n, int es, int tile =
   const long long f = (long long)tile * update_ld(n, es) + (long long)n * update_ld(tile, es);
   return a > f ? a : f;
 }
+// streamed (non-resident) sweeps: Y, Z1, Z2 (n x sweep_ldy) and the chunk buffer
+// Cc (n x sweep_ldc >= kTile x (n + 1) for the triangular panels), dv (kTile)
+__host__ __device__ inline int sweep_ldy(int mc) { return mc + 4; }
+constexpr int kSweepLdc = kTile + 4;   // 4 (mod 16) doubles: conflict-free DMMA fragments
 __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
   const int mc = min_i(m, kMC);
-  return 3LL * n * (mc + 1) + (long long)n * (kTile + 1) + kTile;
+  const long long cc = (long long)n * kSweepLdc > (long long)kTile * (n + 1) ? (long long)n * kSweepLdc
+                                                                           : (long long)kTile * (n + 1);
+  return 3LL * n * sweep_ldy(mc) + cc + kTile;
 }
 
 // ---------------------------------------------------------------------------
 // k_node: 256 threads per level node i.
 //   C_i = chol(L_i)  (potrf, K2)  fused with  C_i V = RHS for the node's
 //   vectors: rows of the right slot (-> F), columns of the left slot (-> G)
-//   and, with WITH_Y, the columns of y_i, in passes of node_chunk(n) vectors
+//   and, with WITH_Y, the columns of y_i, in passes of node_chunk(n, es) vectors
 //   (the first pass factors, later passes reuse the factor).
 // ---------------------------------------------------------------------------
 // INV: also solve C_i W = I and keep W = C_i^{-1} in the strict upper
@@ -234,7 +243,7 @@ __global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
   if (node_uses_gemm(p.n))
     node_gemm_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw);
   else
-    node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n));
+    node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n, sizeof(T)));
 }
 
 // ---------------------------------------------------------------------------
@@ -378,11 +387,146 @@ __device__ __forceinline__ void update_full_body(const Problem<T>& p, const Leve
   }
 }
 
+// ---------------------------------------------------------------------------
+// Whole-block update for 64 < n <= 128 (same tasks as update_full_body): one
+// CTA of 256 threads per target / fill-in block, K streamed through shared
+// memory in kBigKC-column chunks (target: A = [F | G^T], B = A; fill-in:
+// A = F, B(c, k) = G[k][c]), and each warp keeping the accumulators of up to
+// kBigTiles 16 x 32 DMMA tiles of the n x n output (lower tiles only for a
+// target) in registers across the chunks; float operands are widened (exact
+// products, FP64 sums, one rounding per entry).
+// ---------------------------------------------------------------------------
+constexpr int kBigMaxN = 128;
+constexpr int kBigKC = 32;
+constexpr int kBigLd = kBigKC + 4;   // 4 (mod 16) doubles: conflict-free fragments
+constexpr int kBigTiles = 4;         // (128/16) x (128/32) = 32 tiles over 8 warps
+__host__ __device__ inline long long smem_update_big_elems(int n) { return 2LL * n * kBigLd; }
+__host__ __device__ inline bool update_uses_big(int n) { return n > kNodeGemmMaxN && n <= kBigMaxN; }
+
+template <typename T>
+__device__ __forceinline__ void update_big_body(const Problem<T>& p, const Level& lv, int b, int task,
+                                                unsigned char* smem_raw) {
+  const int n = p.n, N = p.N, s = lv.s;
+  const int U = N / (2 * s);
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + n * kBigLd;
+  const bool target = task < U;
+  const T *F, *G;
+  T* Out;
+  int K;
+  if (target) {
+    const int u = task + 1, j = 2 * s * u - 1;
+    F = p.Eb(b, lv.oc + 2 * (u - 1));
+    G = j + s < N ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
+    Out = p.Lb(b, j);
+    K = G ? 2 * n : n;
+  } else {
+    const int t = task - U + 1, i = s - 1 + 2 * s * t;
+    if (i + s >= N) return;
+    F = p.Eb(b, lv.oc + 2 * t);
+    G = p.Eb(b, lv.oc + 2 * t - 1);
+    Out = p.Eb(b, lv.on + t - 1);
+    K = n;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int tm = (n + 15) / 16, tn = (n + 31) / 32;
+  // this warp's tiles: the warp-th, (warp + nw)-th, ... tile of the (lower) tile list
+  int tr[kBigTiles], tc[kBigTiles];
+  int nt = 0;
+  {
+    int idx = 0;
+    for (int i = 0; i < tm; ++i)
+      for (int j = 0; j < tn; ++j) {
+        if (target && 32 * j > 16 * i + 15) continue;
+        if (idx % nw == warp && nt < kBigTiles) {
+          tr[nt] = i * 16;
+          tc[nt] = j * 32;
+          ++nt;
+        }
+        ++idx;
+      }
+  }
+  double acc[kBigTiles][2][4][2];
+#pragma unroll
+  for (int q = 0; q < kBigTiles; ++q)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[q][i][j][0] = acc[q][i][j][1] = 0.0;
+  const T* Bsrc = target ? As : Bs;
+  for (int k0 = 0; k0 < K; k0 += kBigKC) {
+    const int kw = min_i(kBigKC, K - k0);
+    __syncthreads();
+    // A chunk: A(r, k0 + kk) = F[r][k0+kk] (k < n) or G[k0+kk-n][r]; reads
+    // run along rows of F, or along rows of G for a chunk that lies in G
+    if (k0 >= n) {
+      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
+        const int kk = e / n, r = e - kk * n;
+        As[r * kBigLd + kk] = kk < kw ? G[(long long)(k0 + kk - n) * n + r] : T(0);
+      }
+    } else {
+      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
+        const int r = e / kBigKC, kk = e - r * kBigKC, k = k0 + kk;
+        T v = T(0);
+        if (kk < kw) v = k < n ? F[(long long)r * n + k] : G[(long long)(k - n) * n + r];
+        As[r * kBigLd + kk] = v;
+      }
+    }
+    if (!target)
+      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
+        const int kk = e / n, c = e - kk * n, k = k0 + kk;
+        Bs[c * kBigLd + kk] = kk < kw ? G[(long long)k * n + c] : T(0);
+      }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kBigTiles; ++q) {
+      if (q >= nt) break;
+      int ra[2], cb[4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) ra[i] = min_i(tr[q] + 8 * i + g, n - 1);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) cb[j] = min_i(tc[q] + 8 * j + g, n - 1);
+#pragma unroll 2
+      for (int kq = 0; kq < kBigKC; kq += 4) {
+        const int kk = kq + tq;
+        double a[2], bb[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) a[i] = (double)As[ra[i] * kBigLd + kk];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bb[j] = (double)Bsrc[cb[j] * kBigLd + kk];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[q][i][j][0], acc[q][i][j][1], a[i], bb[j]);
+      }
+    }
+  }
+  // epilogue: Out -= D (lower triangle for a target)
+#pragma unroll
+  for (int q = 0; q < kBigTiles; ++q) {
+    if (q >= nt) break;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = tr[q] + 8 * i + g, c = tc[q] + 8 * j + 2 * tq + e;
+          if (r < n && c < n && (!target || c <= r)) {
+            T* o = Out + (long long)r * n + c;
+            *o = (T)((double)*o - acc[q][i][j][e]);
+          }
+        }
+  }
+}
+
 __host__ __device__ inline bool update_uses_full(int n) { return n <= kNodeGemmMaxN; }
 __host__ __device__ inline int update_launch_tasks(int n, int N, const Level& lv) {
-  return update_uses_full(n) ? update_blocks(N, lv) : update_tiles(n, N, lv);
+  return (update_uses_full(n) || update_uses_big(n)) ? update_blocks(N, lv) : update_tiles(n, N, lv);
 }
 __host__ __device__ inline long long smem_update_launch_elems(int n, int es, int tile = kTile) {
+  if (update_uses_big(n)) return smem_update_big_elems(n);
   return update_uses_full(n) ? smem_update_full_elems(n, es) : smem_update_elems(n, es, tile);
 }
 
@@ -401,15 +545,33 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
     update_body<T>(p, lv, b, task, smem_raw);
 }
 
+// 64 < n <= 128: whole-block update (its own kernel: its register-held
+// accumulators would lower the occupancy of the small-block update)
+template <typename T>
+__global__ void __launch_bounds__(256, 1) k_update_big(Problem<T> p, Level lv) {
+  const int per_b = update_blocks(p.N, lv);
+  const int b = blockIdx.x / per_b;
+  const int task = blockIdx.x - b * per_b;
+  pdl_wait();
+  pdl_trigger();
+  if (!p.active(b)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  update_big_body<T>(p, lv, b, task, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // Sweeps.  Shared layout: Y, Z1, Z2 (n x (mc+1) each), Cc (n x (kTile+1)), dv (kTile)
 // ---------------------------------------------------------------------------
 
 // Y -= op(M) Z with M an n x n global block, streamed through Cc in kTile
 // chunks of the contraction index.  TRANS: out[r][c] = sum_k M[k][r] Z[k][c].
+// Each chunk's product runs on the FP64 tensor cores (DMMA warp tiles of
+// 16 x 32; float operands widened in registers, FP64 sums, one rounding per
+// entry and chunk): with n > 64 and many right-hand sides these products, not
+// the block loads, bound the sweep.
 template <typename T, bool TRANS>
 __device__ void sweep_accumulate(T* Y, const T* Z, int ldy, int mc, const T* __restrict__ M, int n, T* Cc) {
-  constexpr int ldc = kTile + 1;
+  constexpr int ldc = kSweepLdc;
   for (int k0 = 0; k0 < n; k0 += kTile) {
     const int kw = min_i(kTile, n - k0);
     __syncthreads();
@@ -419,8 +581,10 @@ __device__ void sweep_accumulate(T* Y, const T* Z, int ldy, int mc, const T* __r
       async_load(Cc, ldc, M + k0, n, kw, n);                   // Cc[r][kk] = M[r][k0+kk]
     cp_async_wait_all();
     __syncthreads();
-    smem_gemm<T, 2, 1, false, false>(n, mc, kw, Cc, ldc, Z + k0 * ldy, ldy,
-                                     [&](int r, int c, T v) { Y[r * ldy + c] -= v; });
+    warp_gemm_dmma<T, false, false>(n, mc, kw, Cc, ldc, Z + k0 * ldy, ldy, [&](int r, int c, double v) {
+      T* o = Y + r * ldy + c;
+      *o = (T)((double)*o - v);
+    });
   }
   __syncthreads();
 }
@@ -837,16 +1001,16 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
     F = p.Eb(b, lv.op + 2 * u - 2);
     if (j + h < N) G = p.Eb(b, lv.op + 2 * u - 1);
   }
-  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : mcmax + 1;
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : sweep_ldy(mcmax);
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
-  T* Ms = Z2 + n * ldy;   // RES: C, F, G (n x ldm each), dv (n); else Cc (n x (kTile+1)), dv
+  T* Ms = Z2 + n * ldy;   // RES: C, F, G (n x ldm each), dv (n); else Cc (smem_sweep_elems), dv
   const int ldm = res_ldm(n);
   T* Cs = Ms;
   T* Fs = Cs + n * ldm;
   T* Gs = Fs + n * ldm;
-  T* dv = RES ? Gs + n * ldm : Ms + n * (kTile + 1);
+  T* dv = RES ? Gs + n * ldm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
   T* yj = p.Xb(b, j);
   const T* Lj = p.Lb(b, j);
   if (!lv.pre) pdl_wait();
@@ -918,7 +1082,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
                                          unsigned char* smem_raw) {
   const int n = p.n, s = lv.s, N = p.N;
   const int i = s - 1 + 2 * s * t;
-  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : mcmax + 1;
+  const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : sweep_ldy(mcmax);
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* Z1 = Y + n * ldy;
   T* Z2 = Z1 + n * ldy;
@@ -927,7 +1091,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
   T* Cs = Ms;
   T* Fs = Cs + n * ldm;
   T* Gs = Fs + n * ldm;
-  T* dv = RES ? Gs + n * ldm : Ms + n * (kTile + 1);
+  T* dv = RES ? Gs + n * ldm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
   const bool right = i + s < N, left = i >= s;
   const T* F = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
   const T* G = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;

@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
 // the ragged kernel reserves for these bodies (its persistent grid is sized
 // with it); they use less (smem_ref_init_elems, smem_residual_x_elems).
 // ---------------------------------------------------------------------------
-constexpr int kResRowMaxN = 64;
+constexpr int kResRowMaxN = 128;
 __host__ __device__ inline long long smem_residual_rows_elems(int n) { return 3LL * n * (n + 1) + 27LL * n; }
 __host__ __device__ inline bool residual_uses_rows(int n) { return n <= kResRowMaxN; }
 
@@ -351,7 +351,11 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
 }
 
 // threads of k_residual_rows: one warp per 8-row tile
-__host__ __device__ inline int residual_rows_threads(int n, int) { return 32 * ((n + 7) / 8); }
+// (at most 256: warps loop over the 8-row tiles of larger blocks)
+__host__ __device__ inline int residual_rows_threads(int n, int) {
+  const int t = 32 * ((n + 7) / 8);
+  return t < 256 ? t : 256;
+}
 
 template <bool REFINE>
 __global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
@@ -368,7 +372,7 @@ __global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
 // float copies of L_i and slot i, R32 = b_i, x_i = 0, ||b||_inf and the row
 // sums of |Psi| over block row i.  One streaming pass, no staging: warp w
 // takes rows w, w + nw, ... of L_i, E_{i-1} and E_i with coalesced loads
-// (lane owns columns lane and lane + 32), writes the float copies, reduces
+// (lane owns columns lane, lane + 32, ...), writes the float copies, reduces
 // the row part of each row sum (lower(D) row, E_{i-1} row) with shuffles and
 // keeps per-lane column partials for the transposed parts (strict lower(D)
 // columns, E_i columns).  The warps' column partials are added in warp order
@@ -402,11 +406,14 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
     a.x[vo + e] = 0.0;
     bmax = fmax(bmax, fabs(v));
   }
-  double cl[2] = {0.0, 0.0}, ce[2] = {0.0, 0.0};
-  for (int r = warp; r < n; r += nw) {
-    double vl[2], vm[2], vp[2];
+  constexpr int H = kResRowMaxN / 32;   // columns per lane
+  double cl[H], ce[H];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < H; ++h) cl[h] = ce[h] = 0.0;
+  for (int r = warp; r < n; r += nw) {
+    double vl[H], vm[H], vp[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
       const int c = lane + 32 * h;
       const bool ok = c < n;
       const int o = r * n + (ok ? c : 0);
@@ -416,7 +423,7 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
     }
     double part = 0.0;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < H; ++h) {
       const int c = lane + 32 * h;
       if (c < n) {
         L32[r * n + c] = (float)vl[h];
@@ -430,7 +437,7 @@ __device__ __forceinline__ void ref_init_rows_body(const RefineArgs& a, int bi, 
     if (lane == 0) rs[r] = part;
   }
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < H; ++h) {
     const int c = lane + 32 * h;
     if (c < n) {
       colp[(warp * 2 + 0) * n + c] = cl[h];

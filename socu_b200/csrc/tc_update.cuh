@@ -39,12 +39,13 @@ __host__ __device__ inline bool update_tc_ok(int n) { return n >= 1 && n <= kTcM
 // Error word of the tensor-core kernels (1: a wait ran out); one per device.
 __device__ int g_tc_error;
 
-// Stage columns [k0, k0 + kTcKC) of a rows x K operand into hi/lo planes.
-// val(r, k) gives the element (only called for r < rows, k < K); the rest is 0.
-template <class Val>
-__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int rows_pad, int rows, int K,
-                                         int k0, Val val) {
-  constexpr int kq = kTcKC / 4;                        // 4-column groups per chunk
+// Stage columns [k0, k0 + KC) of a rows x K operand into hi/lo planes of a
+// KC-column chunk.  val(r, k) gives the element (only called for r < rows,
+// k < K); the rest is 0.  A warp writes 8 rows x 4 columns: conflict-free.
+template <int KC, class Val>
+__device__ __forceinline__ void tc_stage_kc(unsigned char* hi, unsigned char* lo, int rows_pad, int rows, int K,
+                                            int k0, Val val) {
+  constexpr int kq = KC / 4;                           // 4-column groups per chunk
   const int units = (rows_pad / 8) * kq;               // 8 x 4 units
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int u = warp; u < units; u += nw) {
@@ -52,8 +53,14 @@ __device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, i
     const int kk = (u % kq) * 4 + (lane & 3);
     const int k = k0 + kk;
     const float v = (r < rows && k < K) ? val(r, k) : 0.0f;
-    tc::put_split(hi, lo, r, kk, kTcKC, v);
+    tc::put_split(hi, lo, r, kk, KC, v);
   }
+}
+
+template <class Val>
+__device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, int rows_pad, int rows, int K,
+                                         int k0, Val val) {
+  tc_stage_kc<kTcKC>(hi, lo, rows_pad, rows, K, k0, val);
 }
 
 // One update task (see the file comment), all threads of the CTA (multiple
@@ -167,52 +174,57 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(Problem<float> p, Level lv
 }
 
 // ---------------------------------------------------------------------------
-// Level node of a FLOAT factor (n <= 64) with its products on the tcgen05
+// Level node of a FLOAT factor (n <= 128) with its products on the tcgen05
 // tensor cores.  The factor part is the inverse-first node's (node_gemm_body:
 // blocked Cholesky of L_i against the identity, C W = I, W = C^{-1}); the
 // three products that follow -- F = R W^T (right slot), G = W Lf (left slot),
-// y = W y (factor_and_solve) -- share the operand W and run as one MMA group
+// y = W y (factor_and_solve) -- share the operand W and run as MMA groups of
 //     D (n x NB) = W * Bm^T,   Bm rows: the n rows of R, the n columns of Lf,
-//                              the m columns of y  (NB = nr + nl + m <= 256)
-// so D's first n columns hold F^T, the next n G and the last m W y.
+//                              the m columns of y  (NB = nr + nl + m)
+// in column groups of at most 256, so D's columns hold F^T, G and W y.
 // socu: trsm_rltn / trsm_llnn (K3/K4) and the fused forward step,
 // socu/block_tridiag_solver.py:219-279, :108-110, done here as products with
-// the explicit inverse.  The MMA has M = 64 rows (rows n..63 of W are zero):
-// row r of D sits in TMEM lane 32 (r / 16) + r % 16.
+// the explicit inverse.  M = 64 rows for n <= 64 (row r of D in TMEM lane
+// 32 (r / 16) + r % 16), else M = 128 (row r in lane r); rows n..M-1 of W are
+// zero.  K is staged in chunks of 16 columns.  Shared memory: W, then one
+// region that holds the factor's input block S1 and, once C has been written
+// out, the A planes, then the B planes of one column group (52 KB at n = 64:
+// four CTAs per SM, as for the SIMT node).
 // ---------------------------------------------------------------------------
-constexpr int kTcNodeMaxN = 64;
-constexpr int kTcNodeMaxCols = 256;
-__host__ __device__ inline int tc_node_cols(int n, bool right, bool left, int m) {
-  return tc_ncols((right ? n : 0) + (left ? n : 0) + m);
-}
+constexpr int kTcNodeMaxN = 128;
+constexpr int kTcNodeGroup = 256;   // MMA columns per group (TMEM columns allocated)
+constexpr int kTcNodeKC = 16;
+__host__ __device__ inline int tc_node_M(int n) { return n <= 64 ? 64 : 128; }
 __host__ __device__ inline uint32_t tmem_cols_for(int cols) {
   return cols <= 32 ? 32u : (cols <= 64 ? 64u : (cols <= 128 ? 128u : 256u));
 }
-// shared memory: S1, W (n x gemm_ld) for the factor, then the A (64 rows) and
-// B (up to kTcNodeMaxCols rows) hi/lo planes of one K chunk
+__host__ __device__ inline long long round128(long long b) { return ((b + 127) / 128) * 128; }
+__host__ __device__ inline long long smem_node_tc_w(int n) { return round128((long long)n * gemm_ld(n, 4) * 4); }
+__host__ __device__ inline long long smem_node_tc_s1(int n) {
+  const long long s1 = round128((long long)n * gemm_ld(n, 4) * 4), a = 2LL * tc_node_M(n) * kTcNodeKC * 4;
+  return s1 > a ? s1 : a;
+}
 __host__ __device__ inline long long smem_node_tc_bytes(int n, int m) {
-  const long long simt = 2LL * n * gemm_ld(n, 4) * 4;
-  return ((simt + 127) / 128) * 128 + 2LL * 64 * kTcKC * 4 + 2LL * tc_ncols(2 * n + m) * kTcKC * 4;
+  const int nb = tc_ncols(2 * n + m), grp = nb < kTcNodeGroup ? nb : kTcNodeGroup;
+  return smem_node_tc_w(n) + smem_node_tc_s1(n) + 2LL * grp * kTcNodeKC * 4;
 }
-__host__ __device__ inline bool node_tc_ok(int n, int m) {
-  return n >= 1 && n <= kTcNodeMaxN && tc_ncols(2 * n + m) <= kTcNodeMaxCols;
-}
+__host__ __device__ inline bool node_tc_ok(int n, int m) { return n >= 1 && n <= kTcNodeMaxN && m >= 0; }
 
-template <bool WITH_Y, bool INV>
+template <bool WITH_Y, bool INV, int KC>
 __device__ __forceinline__ void node_tc_body(const Problem<float>& p, const Level& lv, int b, int t,
                                              unsigned char* smem, uint32_t tmem, uint64_t* bar, unsigned* phase) {
   const int n = p.n, s = lv.s, i = s - 1 + 2 * s * t;
   const bool right = i + s < p.N, left = t >= 1;
   const int ld = gemm_ld(n, 4);
-  float* S1 = reinterpret_cast<float*>(smem);
-  float* W = S1 + n * ld;
-  const long long simt = 2LL * n * ld * 4;
-  unsigned char* a_hi = smem + ((simt + 127) / 128) * 128;
-  unsigned char* a_lo = a_hi + 64 * kTcKC * 4;
-  unsigned char* b_hi = a_lo + 64 * kTcKC * 4;
+  const int M = tc_node_M(n);
+  float* W = reinterpret_cast<float*>(smem);
+  unsigned char* region1 = smem + smem_node_tc_w(n);
+  float* S1 = reinterpret_cast<float*>(region1);           // factor input / C ...
+  unsigned char* a_hi = region1;                          // ... then the A planes
+  unsigned char* a_lo = a_hi + M * KC * 4;
+  unsigned char* b_hi = region1 + smem_node_tc_s1(n);
   const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0;
-  const int NB = nr + nl + ny, NBp = tc_ncols(NB);
-  unsigned char* b_lo = b_hi + NBp * kTcKC * 4;
+  const int NB = nr + nl + ny;
   float* Li = p.Lb(b, i);
   float* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
   float* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
@@ -233,56 +245,69 @@ __device__ __forceinline__ void node_tc_body(const Problem<float>& p, const Leve
     const int r = e / n, c = e - r * n;
     Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : 0.0f);
   }
-  if (NB == 0) return;
-  // products on the tensor cores, K = n in chunks of kTcKC
-  for (int k0 = 0; k0 < n; k0 += kTcKC) {
-    tc_stage(a_hi, a_lo, 64, n, n, k0, [&](int r, int k) { return W[r * ld + k]; });
-    tc_stage(b_hi, b_lo, NBp, NB, n, k0, [&](int c, int k) {
-      if (c < nr) return R[(long long)c * n + k];
-      if (c < nr + nl) return Lf[(long long)k * n + (c - nr)];
-      return yi[(long long)k * m + (c - nr - nl)];
-    });
-    tc::fence_async_smem();
+  __syncthreads();   // S1's space becomes the A planes
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3, parts = blockDim.x / 128, h = warp >> 2;
+  // rows of D held by this warp's sub-partition: M = 64 -> 16 q .. 16 q + 15
+  // (lanes 0-15), M = 128 -> 32 q .. 32 q + 31
+  const int rows_q = M == 64 ? 16 : 32;
+  const int r = rows_q * q + lane;
+  const bool row_ok = lane < rows_q && r < n;
+  for (int g0 = 0; g0 < NB; g0 += kTcNodeGroup) {
+    const int NBg = min_i(kTcNodeGroup, NB - g0), NBgp = tc_ncols(NBg);
+    unsigned char* b_lo = b_hi + NBgp * KC * 4;
+    for (int k0 = 0; k0 < n; k0 += KC) {
+      tc_stage_kc<KC>(a_hi, a_lo, M, n, n, k0, [&](int rr, int k) { return W[rr * ld + k]; });
+      tc_stage_kc<KC>(b_hi, b_lo, NBgp, NBg, n, k0, [&](int cl, int k) {
+        const int c = g0 + cl;
+        if (c < nr) return R[(long long)c * n + k];
+        if (c < nr + nl) return Lf[(long long)k * n + (c - nr)];
+        return yi[(long long)k * m + (c - nr - nl)];
+      });
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (threadIdx.x == 0) {
+        tc::gemm_3xtf32(tmem, tc::saddr(a_hi), tc::saddr(a_lo), tc::saddr(b_hi), tc::saddr(b_lo), NBgp, KC,
+                        k0 > 0 ? 1u : 0u, M);
+        tc::commit(bar);
+      }
+      const bool done = tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+      const bool ok = __syncthreads_and(done) != 0;
+      tc::fence_after_sync();
+      if (!ok) {
+        tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
+        if (threadIdx.x == 0) atomicExch(&g_tc_error, 1);
+        *phase += 1;
+        return;
+      }
+      *phase += 1;
+    }
+    // epilogue of this group: columns split between the blockDim / 128 warps of a quadrant
+    const int span = ((NBgp / 8 + parts - 1) / parts) * 8;
+    const int c_begin = h * span, c_end = min_i(NBg, c_begin + span);
+    if (rows_q * q < n) {
+      for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+        float v[8];
+        tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+        tc::tmem_wait_ld();
+        if (row_ok) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int c = g0 + c0 + e;
+            if (c0 + e >= NBg) break;
+            if (c < nr) R[(long long)c * n + r] = v[e];                    // F[c][r] = D[r][c]
+            else if (c < nr + nl) Lf[(long long)r * n + (c - nr)] = v[e];  // G[r][c - nr]
+            else yi[(long long)r * m + (c - nr - nl)] = v[e];
+          }
+        }
+      }
+    }
+    // the next group overwrites the accumulator: every TMEM read of this one first
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (threadIdx.x == 0) {
-      tc::gemm_3xtf32(tmem, tc::saddr(a_hi), tc::saddr(a_lo), tc::saddr(b_hi), tc::saddr(b_lo), NBp, kTcKC,
-                      k0 > 0 ? 1u : 0u, 64);
-      tc::commit(bar);
-    }
-    const bool done = tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
-    const bool ok = __syncthreads_and(done) != 0;
-    tc::fence_after_sync();
-    if (!ok) {
-      tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
-      if (threadIdx.x == 0) atomicExch(&g_tc_error, 1);
-      *phase += 1;
-      return;
-    }
-    *phase += 1;
-  }
-  // epilogue: warp w reads rows 16 (w % 4) .. +15 (lanes 0-15 of its
-  // sub-partition), columns split between the blockDim / 128 warps of a quadrant
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int q = warp & 3, parts = blockDim.x / 128, h = warp >> 2;
-  const int r = 16 * q + lane;
-  const int span = ((NBp / 8 + parts - 1) / parts) * 8;
-  const int c_begin = h * span, c_end = min_i(NB, c_begin + span);
-  if (16 * q >= n) return;
-  for (int c0 = c_begin; c0 < c_end; c0 += 8) {
-    float v[8];
-    tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
-    tc::tmem_wait_ld();
-    if (lane < 16 && r < n) {
-#pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const int c = c0 + e;
-        if (c < nr) R[(long long)c * n + r] = v[e];                  // F[c][r] = D[r][c]
-        else if (c < nr + nl) Lf[(long long)r * n + (c - nr)] = v[e];  // G[r][c - nr]
-        else if (c < NB) yi[(long long)r * m + (c - nr - nl)] = v[e];
-      }
-    }
   }
 }
 
@@ -295,7 +320,8 @@ __global__ void __launch_bounds__(256, 1) k_node_tc(Problem<float> p, Level lv) 
   const int t = blockIdx.x - b * lv.d;
   if (!p.active(b)) return;
   const int i = lv.s - 1 + 2 * lv.s * t;
-  const uint32_t ncols = tmem_cols_for(tc_node_cols(p.n, i + lv.s < p.N, t >= 1, WITH_Y ? p.m : 0));
+  const int nb = (i + lv.s < p.N ? p.n : 0) + (t >= 1 ? p.n : 0) + (WITH_Y ? p.m : 0);
+  const uint32_t ncols = tmem_cols_for(tc_ncols(nb < kTcNodeGroup ? nb : kTcNodeGroup));
   const int warp = threadIdx.x >> 5;
   if (warp == 0) tc::tmem_alloc(&tbase, ncols);
   if (threadIdx.x == 0) tc::mbar_init(&bar, 1);
@@ -305,7 +331,7 @@ __global__ void __launch_bounds__(256, 1) k_node_tc(Problem<float> p, Level lv) 
   pdl_wait();
   pdl_trigger();
   unsigned phase = 0;
-  node_tc_body<WITH_Y, INV>(p, lv, b, t, smem_raw, tbase, &bar, &phase);
+  node_tc_body<WITH_Y, INV, kTcNodeKC>(p, lv, b, t, smem_raw, tbase, &bar, &phase);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();

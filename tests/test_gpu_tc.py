@@ -83,7 +83,7 @@ def test_tc_update_parity(n, op):
     assert rel < 1e-4, rel
 
 
-@pytest.mark.parametrize("n,m", [(8, 1), (16, 4), (32, 8), (48, 3), (64, 8), (64, 40)])
+@pytest.mark.parametrize("n,m", [(8, 1), (16, 4), (32, 8), (48, 3), (64, 8), (64, 40), (68, 2), (100, 5), (128, 32)])
 @pytest.mark.parametrize("op", ["factor_and_solve", "factor+solve"])
 def test_tc_node_parity(n, m, op):
     """Float level nodes with their products on the tensor cores (node_tensor_cores=1),
