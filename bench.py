@@ -729,6 +729,39 @@ def bench_autograd(dev, steps, time_steps, agg):
             "value": B / sec, "unit": "solves/s (forward + backward)", "ms_per_step": sec * 1e3}
 
 
+NCU_CASES = {
+    # the mixed solve's float factor_and_solve on 4 systems of the workload shape (L, E float: 200 MB > L2)
+    "node": dict(B=4, N=1024, n=64, m=8, shift=10.0),
+    # the stress block size at a reduced horizon (FP64 blocks ~0.8 GB)
+    "stress": dict(B=1, N=2048, n=128, m=32, shift=24.0),
+}
+
+
+def run_ncu_case(name):
+    """Small eager workloads for ncu captures of single kernels (not a bench
+    line): two factor_and_solve runs in float and two in FP64 of the case's
+    shape, then one mixed solve without its CUDA graph (ncu does not report
+    kernels inside conditional graph nodes)."""
+    import torch
+
+    from socu_b200.block_tridiag_solver import create_cholesky_factor_and_solve_launch
+    from socu_b200.mixed import create_cholesky_refined_solve_launch
+    from socu_b200.problems import readme_blocks
+
+    c = NCU_CASES[name]
+    L, E, b = readme_blocks(c["N"], c["n"], c["m"], shift=c["shift"], seed=SEED, batch=c["B"], device="cuda")
+    for dt in (torch.float32, torch.float64):
+        for _ in range(2):
+            Lw, Ew, xw = L.to(dt), E.to(dt), b.to(dt)
+            create_cholesky_factor_and_solve_launch(Lw, Ew, xw, dtype=dt)()
+            torch.cuda.synchronize()
+    x = torch.zeros_like(b)
+    run = create_cholesky_refined_solve_launch(L, E, b, x, tol=TOL, max_iter=3, use_cuda_graph=False)
+    run()
+    torch.cuda.synchronize()
+    print(json.dumps({"ncu_case": name, **c, "eta_max": float(run.eta.max())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -739,7 +772,12 @@ def main():
                     help="omit the stress, ragged-batch and autograd measurements")
     ap.add_argument("--profile", action="store_true",
                     help="for profiler runs only: the mixed solve runs without its CUDA graph")
+    ap.add_argument("--ncu-case", choices=sorted(NCU_CASES), default=None,
+                    help="run a small eager workload for ncu kernel captures instead of the benchmark")
     args = ap.parse_args()
+    if args.ncu_case:
+        run_ncu_case(args.ncu_case)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

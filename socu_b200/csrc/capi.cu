@@ -375,6 +375,27 @@ struct Fork {
   }
 };
 
+// Block-row FP64 residual (n <= 128): 1, 2 or 4 eight-column groups of
+// right-hand sides per pass over the matrix blocks, by n_rhs.
+template <bool REFINE>
+cudaError_t launch_residual_rows(const RefineArgs& a, cudaStream_t st, bool pdl) {
+  const int gr = residual_groups(a.m);
+  const size_t smem = smem_residual_x_elems(a.n, gr) * sizeof(double);
+  const unsigned blocks = (unsigned)((long long)a.B * a.N), threads = (unsigned)residual_rows_threads(a.n, a.m);
+  cudaError_t e;
+  if (gr == 1) {
+    e = prepare(k_residual_rows<REFINE, 1>, smem);
+    if (e == cudaSuccess) launch(k_residual_rows<REFINE, 1>, blocks, threads, smem, st, pdl, a);
+  } else if (gr == 2) {
+    e = prepare(k_residual_rows<REFINE, 2>, smem);
+    if (e == cudaSuccess) launch(k_residual_rows<REFINE, 2>, blocks, threads, smem, st, pdl, a);
+  } else {
+    e = prepare(k_residual_rows<REFINE, 4>, smem);
+    if (e == cudaSuccess) launch(k_residual_rows<REFINE, 4>, blocks, threads, smem, st, pdl, a);
+  }
+  return e;
+}
+
 // Enqueue (or count, when st == nullptr and count != nullptr) the kernels of one op.
 // inv: the factor carries (FACTOR, FACTOR_AND_SOLVE) or has (SOLVE) its
 // diagonal inverses; only for internal factors or within factor_and_solve.
@@ -713,8 +734,7 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     prof_end(st);
     prof_begin(st, SOCU_KIND_RESIDUAL);
     if (residual_uses_rows(a.n))
-      launch(k_residual_rows<true>, (unsigned)((long long)a.B * a.N), (unsigned)residual_rows_threads(a.n, a.m),
-             smem_residual_x_elems(a.n) * sizeof(double), st, pdl, a);
+      launch_residual_rows<true>(a, st, pdl);
     else
       launch(k_residual<true>, (unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
              st, pdl, a);
@@ -834,8 +854,7 @@ int capture_fallback(const RefineArgs& a, const FallbackArgs& f, cudaStream_t ca
   ra.active = f.fb;
   if (st == SOCU_OK) {
     if (residual_uses_rows(a.n))
-      k_residual_rows<true><<<(unsigned)((long long)a.B * a.N), residual_rows_threads(a.n, a.m),
-                              smem_residual_x_elems(a.n) * sizeof(double), body>>>(ra);
+      launch_residual_rows<true>(ra, body, false);
     else
       k_residual<true><<<(unsigned)((long long)a.B * a.N * ceil_div(a.n, kResRows)), 256,
                          smem_residual_elems(a.n) * sizeof(double), body>>>(ra);
@@ -1518,9 +1537,8 @@ int socu_block_tridiag_residual(const double* L, const double* E, const double* 
   a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
   const size_t sres = smem_residual_elems(d.n) * sizeof(double);
   if (residual_uses_rows(d.n)) {
-    k_residual_rows<false><<<(unsigned)((long long)d.B * d.N), residual_rows_threads(d.n, d.m),
-                             smem_residual_x_elems(d.n) * sizeof(double),
-                             static_cast<cudaStream_t>(stream)>>>(a);
+    e = launch_residual_rows<false>(a, static_cast<cudaStream_t>(stream), false);
+    if (e != cudaSuccess) return cuda_status(e);
   } else {
     e = prepare(k_residual<false>, sres);
     if (e != cudaSuccess) return cuda_status(e);

@@ -37,10 +37,9 @@ __host__ __device__ inline int min_i(int a, int b) { return a < b ? a : b; }
 // shared-memory sizes (elements) ------------------------------------------------
 __host__ __device__ inline int gemm_ld(int n, int es) { return es == 8 ? ((n + 15) / 16) * 16 + 4 : n + 1; }
 // vectors solved per pass of k_node (items beyond the block size loop)
-// (n > 64: as many as fit beside the n x n block in 227 KB -- all 2n + 32 of
-// a 128-block node with 32 right-hand sides in one pass for float, 80 per pass
-// for double)
-__host__ __device__ inline int node_chunk(int n, int es) { return n <= 64 ? 232 : (es == 4 ? 304 : 80); }
+// (n > 64: 64 for float -- two CTAs per SM, measured faster than one pass of
+// all vectors at one CTA per SM -- and 80 for double, the most that fit)
+__host__ __device__ inline int node_chunk(int n, int es) { return n <= 64 ? 232 : (es == 4 ? 64 : 80); }
 __host__ __device__ inline long long smem_node_elems(int n, int es) {
   return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n, es), es);
 }
@@ -55,10 +54,16 @@ __host__ __device__ inline long long smem_update_elems(int n, int es, int tile =
 // Cc (n x sweep_ldc >= kTile x (n + 1) for the triangular panels), dv (kTile)
 __host__ __device__ inline int sweep_ldy(int mc) { return mc + 4; }
 constexpr int kSweepLdc = kTile + 4;   // 4 (mod 16) doubles: conflict-free DMMA fragments
+
+// cp.async groups: close the group of copies issued so far / wait until at
+// most one group is still in flight
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+// (two chunk buffers: the next chunk's copies overlap this chunk's product)
 __host__ __device__ inline long long smem_sweep_elems(int n, int m) {
   const int mc = min_i(m, kMC);
-  const long long cc = (long long)n * kSweepLdc > (long long)kTile * (n + 1) ? (long long)n * kSweepLdc
-                                                                           : (long long)kTile * (n + 1);
+  const long long cc = 2LL * n * kSweepLdc > (long long)kTile * (n + 1) ? 2LL * n * kSweepLdc
+                                                                        : (long long)kTile * (n + 1);
   return 3LL * n * sweep_ldy(mc) + cc + kTile;
 }
 
@@ -400,7 +405,8 @@ constexpr int kBigMaxN = 128;
 constexpr int kBigKC = 32;
 constexpr int kBigLd = kBigKC + 4;   // 4 (mod 16) doubles: conflict-free fragments
 constexpr int kBigTiles = 4;         // (128/16) x (128/32) = 32 tiles over 8 warps
-__host__ __device__ inline long long smem_update_big_elems(int n) { return 2LL * n * kBigLd; }
+// two chunk buffers (A and B each): the next chunk's copies overlap this chunk's products
+__host__ __device__ inline long long smem_update_big_elems(int n) { return 4LL * n * kBigLd; }
 __host__ __device__ inline bool update_uses_big(int n) { return n > kNodeGemmMaxN && n <= kBigMaxN; }
 
 template <typename T>
@@ -408,8 +414,7 @@ __device__ __forceinline__ void update_big_body(const Problem<T>& p, const Level
                                                 unsigned char* smem_raw) {
   const int n = p.n, N = p.N, s = lv.s;
   const int U = N / (2 * s);
-  T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + n * kBigLd;
+  T* buf = reinterpret_cast<T*>(smem_raw);   // [2][A | B], each n x kBigLd
   const bool target = task < U;
   const T *F, *G;
   T* Out;
@@ -428,6 +433,43 @@ __device__ __forceinline__ void update_big_body(const Problem<T>& p, const Level
     Out = p.Eb(b, lv.on + t - 1);
     K = n;
   }
+  // asynchronous copies of chunk c (columns [32c, 32c + 32) of A and B) into
+  // buffer c & 1; columns past K are zero-filled with plain stores
+  auto stage = [&](int c) {
+    T* As = buf + (c & 1) * 2 * n * kBigLd;
+    T* Bs = As + n * kBigLd;
+    const int k0 = c * kBigKC, kw = min_i(kBigKC, K - k0);
+    if (k0 + kw <= n) {
+      // A(r, kk) = F[r][k0 + kk]: rows of F
+      for (int e = threadIdx.x; e < n * kw; e += blockDim.x) {
+        const int r = e / kw, kk = e - r * kw;
+        cp_async_elem(As + r * kBigLd + kk, F + (long long)r * n + k0 + kk);
+      }
+    } else if (k0 >= n) {
+      // A(r, kk) = G[k0 + kk - n][r]: rows of G, transposed
+      for (int e = threadIdx.x; e < n * kw; e += blockDim.x) {
+        const int kk = e / n, r = e - kk * n;
+        cp_async_elem(As + r * kBigLd + kk, G + (long long)(k0 + kk - n) * n + r);
+      }
+    } else {
+      for (int e = threadIdx.x; e < n * kw; e += blockDim.x) {
+        const int r = e / kw, kk = e - r * kw, k = k0 + kk;
+        cp_async_elem(As + r * kBigLd + kk, k < n ? F + (long long)r * n + k : G + (long long)(k - n) * n + r);
+      }
+    }
+    if (!target)   // B(c, kk) = G[k0 + kk][c]
+      for (int e = threadIdx.x; e < n * kw; e += blockDim.x) {
+        const int kk = e / n, cc = e - kk * n;
+        cp_async_elem(Bs + cc * kBigLd + kk, G + (long long)(k0 + kk) * n + cc);
+      }
+    if (kw < kBigKC)
+      for (int e = threadIdx.x; e < n * (kBigKC - kw); e += blockDim.x) {
+        const int r = e / (kBigKC - kw), kk = kw + e - r * (kBigKC - kw);
+        As[r * kBigLd + kk] = T(0);
+        if (!target) Bs[r * kBigLd + kk] = T(0);
+      }
+    cp_async_commit();
+  };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, tq = lane & 3;
   const int tm = (n + 15) / 16, tn = (n + 31) / 32;
@@ -454,31 +496,15 @@ __device__ __forceinline__ void update_big_body(const Problem<T>& p, const Level
     for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[q][i][j][0] = acc[q][i][j][1] = 0.0;
-  const T* Bsrc = target ? As : Bs;
-  for (int k0 = 0; k0 < K; k0 += kBigKC) {
-    const int kw = min_i(kBigKC, K - k0);
+  const int chunks = (K + kBigKC - 1) / kBigKC;
+  stage(0);
+  for (int c = 0; c < chunks; ++c) {
+    if (c + 1 < chunks) stage(c + 1);
+    else cp_async_commit();       // empty group: wait_group 1 then covers chunk c
+    cp_async_wait_one();
     __syncthreads();
-    // A chunk: A(r, k0 + kk) = F[r][k0+kk] (k < n) or G[k0+kk-n][r]; reads
-    // run along rows of F, or along rows of G for a chunk that lies in G
-    if (k0 >= n) {
-      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
-        const int kk = e / n, r = e - kk * n;
-        As[r * kBigLd + kk] = kk < kw ? G[(long long)(k0 + kk - n) * n + r] : T(0);
-      }
-    } else {
-      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
-        const int r = e / kBigKC, kk = e - r * kBigKC, k = k0 + kk;
-        T v = T(0);
-        if (kk < kw) v = k < n ? F[(long long)r * n + k] : G[(long long)(k - n) * n + r];
-        As[r * kBigLd + kk] = v;
-      }
-    }
-    if (!target)
-      for (int e = threadIdx.x; e < n * kBigKC; e += blockDim.x) {
-        const int kk = e / n, c = e - kk * n, k = k0 + kk;
-        Bs[c * kBigLd + kk] = kk < kw ? G[(long long)k * n + c] : T(0);
-      }
-    __syncthreads();
+    const T* As = buf + (c & 1) * 2 * n * kBigLd;
+    const T* Bsrc = target ? As : As + n * kBigLd;
 #pragma unroll
     for (int q = 0; q < kBigTiles; ++q) {
       if (q >= nt) break;
@@ -501,6 +527,7 @@ __device__ __forceinline__ void update_big_body(const Problem<T>& p, const Level
           for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[q][i][j][0], acc[q][i][j][1], a[i], bb[j]);
       }
     }
+    __syncthreads();   // buffer c & 1 is restaged for chunk c + 2
   }
   // epilogue: Out -= D (lower triangle for a target)
 #pragma unroll
@@ -563,30 +590,49 @@ __global__ void __launch_bounds__(256, 1) k_update_big(Problem<T> p, Level lv) {
 // Sweeps.  Shared layout: Y, Z1, Z2 (n x (mc+1) each), Cc (n x (kTile+1)), dv (kTile)
 // ---------------------------------------------------------------------------
 
-// Y -= op(M) Z with M an n x n global block, streamed through Cc in kTile
-// chunks of the contraction index.  TRANS: out[r][c] = sum_k M[k][r] Z[k][c].
-// Each chunk's product runs on the FP64 tensor cores (DMMA warp tiles of
-// 16 x 32; float operands widened in registers, FP64 sums, one rounding per
-// entry and chunk): with n > 64 and many right-hand sides these products, not
-// the block loads, bound the sweep.
-template <typename T, bool TRANS>
-__device__ void sweep_accumulate(T* Y, const T* Z, int ldy, int mc, const T* __restrict__ M, int n, T* Cc) {
+// Y -= op(M1) Z1 + op(M2) Z2 with M1, M2 n x n global blocks (a null M skips
+// its product), streamed through two Cc buffers in kTile chunks of the
+// contraction index: the copies of chunk c + 1 are in flight while chunk c's
+// product runs.  TRx: op(M)[r][k] = M[k][r].  Each chunk's product runs on the
+// FP64 tensor cores (DMMA warp tiles of 16 x 32; float operands widened in
+// registers, FP64 sums, one rounding per entry and chunk): with n > 64 and
+// many right-hand sides these products, not the block loads, bound the sweep.
+template <typename T, bool TR1, bool TR2>
+__device__ void sweep_accumulate2(T* Y, const T* Z1, const T* __restrict__ M1, const T* Z2,
+                                  const T* __restrict__ M2, int ldy, int mc, int n, T* Cc) {
   constexpr int ldc = kSweepLdc;
-  for (int k0 = 0; k0 < n; k0 += kTile) {
-    const int kw = min_i(kTile, n - k0);
-    __syncthreads();
-    if (TRANS)
-      async_load_t(Cc, ldc, M + (long long)k0 * n, kw, n, n);   // Cc[r][kk] = M[k0+kk][r]
+  const int per = (n + kTile - 1) / kTile;
+  const int c1 = M1 ? per : 0, total = c1 + (M2 ? per : 0);
+  if (total == 0) return;
+  auto stage = [&](int c) {
+    T* dst = Cc + (c & 1) * n * ldc;
+    const bool first = c < c1;
+    const T* M = first ? M1 : M2;
+    const bool tr = first ? TR1 : TR2;
+    const int k0 = (first ? c : c - c1) * kTile, kw = min_i(kTile, n - k0);
+    if (tr)
+      async_load_t(dst, ldc, M + (long long)k0 * n, kw, n, n);   // dst[r][kk] = M[k0+kk][r]
     else
-      async_load(Cc, ldc, M + k0, n, kw, n);                   // Cc[r][kk] = M[r][k0+kk]
-    cp_async_wait_all();
-    __syncthreads();
-    warp_gemm_dmma<T, false, false>(n, mc, kw, Cc, ldc, Z + k0 * ldy, ldy, [&](int r, int c, double v) {
-      T* o = Y + r * ldy + c;
-      *o = (T)((double)*o - v);
-    });
-  }
+      async_load(dst, ldc, M + k0, n, kw, n);                   // dst[r][kk] = M[r][k0+kk]
+    cp_async_commit();
+  };
   __syncthreads();
+  stage(0);
+  for (int c = 0; c < total; ++c) {
+    if (c + 1 < total) stage(c + 1);
+    else cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const bool first = c < c1;
+    const int k0 = (first ? c : c - c1) * kTile, kw = min_i(kTile, n - k0);
+    const T* Z = first ? Z1 : Z2;
+    warp_gemm_dmma<T, false, false>(n, mc, kw, Cc + (c & 1) * n * ldc, ldc, Z + k0 * ldy, ldy,
+                                    [&](int r, int cc, double v) {
+                                      T* o = Y + r * ldy + cc;
+                                      *o = (T)((double)*o - v);
+                                    });
+    __syncthreads();
+  }
 }
 
 // Y <- C^{-1} Y (lower C = lower(Lb)), blocked by kTile rows, warp per column.
@@ -1054,10 +1100,7 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
         res_tri_solve<T, false>(Y, ldy, mc, Cs, ldm, dv, n);
       }
     } else {
-      if (pull) {
-        sweep_accumulate<T, false>(Y, Z1, ldy, mc, F, n, Ms);
-        if (G) sweep_accumulate<T, true>(Y, Z2, ldy, mc, G, n, Ms);
-      }
+      if (pull) sweep_accumulate2<T, false, true>(Y, Z1, F, Z2, G, ldy, mc, n, Ms);
       if (solve) sweep_lower_solve(Y, ldy, mc, Lj, n, Ms, dv);
     }
     store_block(yj + c0, p.m, Y, ldy, n, mc);
@@ -1138,8 +1181,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
       }
       res_tri_solve<T, true>(Y, ldy, mc, Cs, ldm, dv, n);
     } else {
-      if (right) sweep_accumulate<T, true>(Y, Z1, ldy, mc, F, n, Ms);
-      if (left) sweep_accumulate<T, false>(Y, Z2, ldy, mc, G, n, Ms);
+      sweep_accumulate2<T, true, false>(Y, Z1, F, Z2, G, ldy, mc, n, Ms);
       sweep_upper_solve(Y, ldy, mc, Li, n, Ms, dv);
     }
     store_block(xi + c0, p.m, Y, ldy, n, mc);

@@ -344,7 +344,7 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
       }
       case kRgRes: {
         if constexpr (!kPlain) {
-          residual_rows_body<true>(rg_refine_args(a, I, ii), 0, u, smem);
+          residual_rows_body<true, 1>(rg_refine_args(a, I, ii), 0, u, smem);
         }
         break;
       }

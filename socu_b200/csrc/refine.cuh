@@ -245,30 +245,35 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
 // Block-row kernels for n <= kResRowMaxN: one CTA per block row i reads the
 // three blocks of that row, L_i, E_{i-1} and E_i, with coalesced loads
 // (missing neighbours as zeros), so every element of L and E is read from HBM
-// once per row that needs it.  smem_residual_rows_elems is the shared memory
-// the ragged kernel reserves for these bodies (its persistent grid is sized
-// with it); they use less (smem_ref_init_elems, smem_residual_x_elems).
+// once per row that needs it (and per 32 right-hand sides).
 // ---------------------------------------------------------------------------
 constexpr int kResRowMaxN = 128;
-__host__ __device__ inline long long smem_residual_rows_elems(int n) { return 3LL * n * (n + 1) + 27LL * n; }
 __host__ __device__ inline bool residual_uses_rows(int n) { return n <= kResRowMaxN; }
 
 // r_i = b_i - (D_i x_i + E_{i-1} x_{i-1} + E_i^T x_{i+1}) for the whole block
-// row, on FP64 tensor cores (mma.m8n8k4 .f64).  Per chunk of 8 right-hand
-// sides the CTA stages x_{i-1}, x_i, x_{i+1} in shared memory (stride 12:
-// conflict-free B fragments; missing neighbours and columns as zeros); the
-// matrix fragments are read straight from global memory, each element once.
-// Warp task = one 8-row output tile: 3 blocks x ceil(n/4) k-steps into six
-// independent accumulators (block x k parity).  Fragment layout: a0 = A[g][t],
-// b0 = B[t][g], {c0, c1} = C[g][2t + {0, 1}] (g = lane / 4, t = lane % 4).
-// D_i is symmetric from its lower triangle: above the diagonal the transposed
-// element is read.  Any blockDim.x that is a multiple of 32 works.
-// Shared: 3 x n x kResXld doubles (smem_residual_x_elems; the ragged kernel's
-// buffer, sized by smem_residual_rows_elems, is larger).
-constexpr int kResXld = 12;
-__host__ __device__ inline long long smem_residual_x_elems(int n) { return 3LL * n * kResXld; }
-template <bool REFINE>
+// row, on FP64 tensor cores (mma.m8n8k4 .f64).  Per super-chunk of up to 32
+// right-hand sides the CTA stages x_{i-1}, x_i, x_{i+1} in shared memory
+// (stride 36: conflict-free B fragments; missing neighbours and columns as
+// zeros); the matrix fragments are read straight from global memory, each
+// element once per super-chunk, and multiplied into all (up to four) 8-column
+// groups of the chunk.  Warp task = one 8-row output tile: 3 blocks x
+// ceil(n/4) k-steps into independent accumulators (block x k parity x column
+// group).  Fragment layout: a0 = A[g][t], b0 = B[t][g], {c0, c1} = C[g][2t +
+// {0, 1}] (g = lane / 4, t = lane % 4).  D_i is symmetric from its lower
+// triangle: above the diagonal the transposed element is read.  Any
+// blockDim.x that is a multiple of 32 works.
+// Shared: 3 x n x kResXld doubles (smem_residual_x_elems).
+// GR = 8-column groups per super-chunk (1, 2 or 4, by the number of
+// right-hand sides): the super-chunk is 8 GR columns wide, staged with stride
+// 8 GR + 4 doubles (4 mod 16 for GR = 1 and 4; 20 for GR = 2).
+__host__ __device__ inline int residual_groups(int m) { return m <= 8 ? 1 : (m <= 16 ? 2 : 4); }
+__host__ __device__ inline long long smem_residual_x_elems(int n, int gr) { return 3LL * n * (8 * gr + 4); }
+// shared memory the ragged kernel reserves for its residual / set-up phases
+// (doubles): the one-group residual's x staging, which exceeds the set-up's 17 n
+__host__ __device__ inline long long smem_residual_rows_elems(int n) { return smem_residual_x_elems(n, 1); }
+template <bool REFINE, int GR>
 __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, int i, unsigned char* smem_raw) {
+  constexpr int kResXC = 8 * GR, kResXld = kResXC + 4;
   __shared__ double red[32];
   double* const xs0 = reinterpret_cast<double*>(smem_raw);
   const int xstride = a.n * kResXld;   // x_{i-1}, x_i, x_{i+1} chunks back to back
@@ -284,11 +289,12 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
   const int g = lane >> 2, t = lane & 3;
   const int rts = (n + 7) >> 3;
   double rmax = 0.0, xmax = 0.0;
-  for (int c0 = 0; c0 < m; c0 += 8) {
-    const int mc = min(8, m - c0);
+  for (int c0 = 0; c0 < m; c0 += kResXC) {
+    const int mc = min(kResXC, m - c0);
+    const int groups = (mc + 7) >> 3;
     __syncthreads();
-    for (int e = threadIdx.x; e < 3 * n * 8; e += blockDim.x) {
-      const int j = e / (n * 8), rem = e - j * n * 8, k = rem >> 3, c = rem & 7;
+    for (int e = threadIdx.x; e < 3 * n * kResXC; e += blockDim.x) {
+      const int j = e / (n * kResXC), rem = e - j * n * kResXC, k = rem / kResXC, c = rem - k * kResXC;
       const bool ok = c < mc && (j == 1 || (j == 0 ? hasM : hasP));
       xs0[j * xstride + k * kResXld + c] = ok ? x1[(long long)(j - 1) * n * m + (long long)k * m + c0 + c] : 0.0;
     }
@@ -297,9 +303,11 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
       const int r0 = rt * 8, ra = r0 + g;
       const bool rv = ra < n;
       const int rr = rv ? ra : 0;
-      double acc[6][2];
+      double acc[GR][6][2];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) acc[q][0] = acc[q][1] = 0.0;
+      for (int q = 0; q < GR; ++q)
+#pragma unroll
+        for (int u = 0; u < 6; ++u) acc[q][u][0] = acc[q][u][1] = 0.0;
 #pragma unroll 2
       for (int k0 = 0; k0 < n; k0 += 8) {
 #pragma unroll
@@ -312,29 +320,38 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
           const double aD = av ? dv : 0.0;
           const double aM = (av && hasM) ? Em[rr * n + kk] : 0.0;
           const double aP = (av && hasP) ? Ep[kk * n + rr] : 0.0;
-          const int xo = kk * kResXld + g;
-          const double b1 = kv ? xs0[xstride + xo] : 0.0;
-          const double b0 = kv ? xs0[xo] : 0.0;
-          const double b2 = kv ? xs0[2 * xstride + xo] : 0.0;
-          dmma_8x8x4(acc[h][0], acc[h][1], aD, b1);
-          dmma_8x8x4(acc[2 + h][0], acc[2 + h][1], aM, b0);
-          dmma_8x8x4(acc[4 + h][0], acc[4 + h][1], aP, b2);
+#pragma unroll
+          for (int q = 0; q < GR; ++q) {
+            if (q >= groups) break;
+            const int xo = kk * kResXld + 8 * q + g;
+            const double b1 = kv ? xs0[xstride + xo] : 0.0;
+            const double b0 = kv ? xs0[xo] : 0.0;
+            const double b2 = kv ? xs0[2 * xstride + xo] : 0.0;
+            dmma_8x8x4(acc[q][h][0], acc[q][h][1], aD, b1);
+            dmma_8x8x4(acc[q][2 + h][0], acc[q][2 + h][1], aM, b0);
+            dmma_8x8x4(acc[q][4 + h][0], acc[q][4 + h][1], aP, b2);
+          }
         }
       }
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = r0 + g, c = 2 * t + e;
-        if (r < n && c < mc) {
-          const long long o = vi + (long long)r * m + c0 + c;
-          const double y = ((acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e])) + (acc[4][e] + acc[5][e]);
-          const double res = a.b[o] - y;
-          if (REFINE) {
-            a.R32[o] = (float)res;
-            const double xv = xs0[xstride + r * kResXld + c];
-            rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
-            xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
-          } else {
-            a.rout[o] = res;
+      for (int q = 0; q < GR; ++q) {
+        if (q >= groups) break;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = r0 + g, c = 8 * q + 2 * t + e;
+          if (r < n && c < mc) {
+            const long long o = vi + (long long)r * m + c0 + c;
+            const double y = ((acc[q][0][e] + acc[q][1][e]) + (acc[q][2][e] + acc[q][3][e])) +
+                             (acc[q][4][e] + acc[q][5][e]);
+            const double res = a.b[o] - y;
+            if (REFINE) {
+              a.R32[o] = (float)res;
+              const double xv = xs0[xstride + r * kResXld + c];
+              rmax = isfinite(res) ? fmax(rmax, fabs(res)) : __longlong_as_double(0x7ff0000000000000LL);
+              xmax = isfinite(xv) ? fmax(xmax, fabs(xv)) : __longlong_as_double(0x7ff0000000000000LL);
+            } else {
+              a.rout[o] = res;
+            }
           }
         }
       }
@@ -350,22 +367,21 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
   }
 }
 
-// threads of k_residual_rows: one warp per 8-row tile
 // (at most 256: warps loop over the 8-row tiles of larger blocks)
 __host__ __device__ inline int residual_rows_threads(int n, int) {
   const int t = 32 * ((n + 7) / 8);
   return t < 256 ? t : 256;
 }
 
-template <bool REFINE>
-__global__ void __launch_bounds__(256, 4) k_residual_rows(RefineArgs a) {
+template <bool REFINE, int GR>
+__global__ void __launch_bounds__(256, GR == 4 ? 2 : (GR == 2 ? 3 : 4)) k_residual_rows(RefineArgs a) {
   pdl_wait();
   pdl_trigger();
   const int bi = blockIdx.x / a.N;
   const int i = blockIdx.x - bi * a.N;
   if (REFINE && !a.active[bi]) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  residual_rows_body<REFINE>(a, bi, i, smem_raw);
+  residual_rows_body<REFINE, GR>(a, bi, i, smem_raw);
 }
 
 // Refinement set-up for block row i (if i < N) and storage slot i (if i < S):
