@@ -65,6 +65,9 @@ const char* socu_status_string(int status);
 /* The last CUDA error seen by this library in the calling thread (0 if none). */
 int socu_last_cuda_error(void);
 
+/* Diagnostics: the line of the library source that reported that error. */
+int socu_last_cuda_error_line(void);
+
 /* floor(log2(horizon)) + 1, or -1 for horizon <= 0.
  * Replaces calculate_recursive_iterations, socu/block_tridiag_solver.py:12-15. */
 int64_t socu_recursive_iterations(int64_t horizon);

@@ -71,6 +71,7 @@ _SIGNATURES = {
     "socu_version": (ctypes.c_char_p, []),
     "socu_status_string": (ctypes.c_char_p, [_int]),
     "socu_last_cuda_error": (_int, []),
+    "socu_last_cuda_error_line": (_int, []),
     "socu_recursive_iterations": (_i64, [_i64]),
     "socu_off_diag_storage_len": (_i64, [_i64]),
     "socu_max_block_size": (_i64, [_int, _i64]),
@@ -158,5 +159,5 @@ def check(status: int, what: str):
         lib = load()
         detail = STATUS_TEXT.get(status, "unknown status")
         cuda = lib.socu_last_cuda_error()
-        extra = f" (cudaError {cuda})" if status == -2 else ""
+        extra = f" (cudaError {cuda} at capi.cu:{lib.socu_last_cuda_error_line()})" if status == -2 else ""
         raise RuntimeError(f"{what} failed: {detail}{extra}")

@@ -20,12 +20,15 @@ namespace socu {
 namespace {
 
 thread_local int g_last_cuda_error = 0;
+thread_local int g_last_cuda_line = 0;   // source line of the call that reported it (diagnostics)
 
-int cuda_status(cudaError_t e) {
+int cuda_status_line(cudaError_t e, int line) {
   if (e == cudaSuccess) return SOCU_OK;
   g_last_cuda_error = static_cast<int>(e);
+  g_last_cuda_line = line;
   return SOCU_ERR_CUDA;
 }
+#define cuda_status(e) cuda_status_line((e), __LINE__)
 
 // Level schedule of a horizon-N system (socu/block_tridiag_solver.py:869-914),
 // written to a caller array of kMaxLevels entries (no heap: the no-allocation
@@ -733,9 +736,10 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     launch(k_ref_update, (unsigned)upd_blocks, 256, 0, st, pdl, a);
     prof_end(st);
     prof_begin(st, SOCU_KIND_RESIDUAL);
-    if (residual_uses_rows(a.n))
-      launch_residual_rows<true>(a, st, pdl);
-    else
+    if (residual_uses_rows(a.n)) {
+      const cudaError_t e = launch_residual_rows<true>(a, st, pdl);
+      if (e != cudaSuccess) return cuda_status(e);
+    } else
       launch(k_residual<true>, (unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
              st, pdl, a);
     prof_end(st);
@@ -789,11 +793,11 @@ int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
   long long c = 0, cr = 0;
-  const int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
+  int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (s != SOCU_OK) return s;
-  refine_finish_round(a, st, run ? nullptr : &cr);
+  s = refine_finish_round(a, st, run ? nullptr : &cr);
   if (count) *count = c + cr;
-  return SOCU_OK;
+  return s;
 }
 
 // Enqueue (or count) the full mixed solve with a fixed max_iter rounds
@@ -1326,6 +1330,8 @@ const char* socu_status_string(int status) {
 }
 
 int socu_last_cuda_error(void) { return g_last_cuda_error; }
+
+int socu_last_cuda_error_line(void) { return g_last_cuda_line; }
 
 int64_t socu_recursive_iterations(int64_t horizon) {
   if (horizon <= 0) return -1;

@@ -635,11 +635,14 @@ __device__ void sweep_accumulate2(T* Y, const T* Z1, const T* __restrict__ M1, c
   }
 }
 
-// Y <- C^{-1} Y (lower C = lower(Lb)), blocked by kTile rows, warp per column.
+// Y <- C^{-1} Y (lower C = lower(Lb)), blocked by kTile rows: a warp takes
+// four columns at once (lane = row of the panel), so the panel elements are
+// loaded once for four columns and the four substitution chains interleave.
+constexpr int kSolveCols = 4;
 template <typename T>
 __device__ void sweep_lower_solve(T* Y, int ldy, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int ldc = n + 1;  // Cc holds n*(kTile+1) >= kb*(n+1) elements
+  const int ldc = n + 1;  // Cc holds >= kTile * (n + 1) elements
   for (int K = 0; K < n; K += kTile) {
     const int kb = min_i(kTile, n - K);
     __syncthreads();
@@ -648,30 +651,44 @@ __device__ void sweep_lower_solve(T* Y, int ldy, int mc, const T* __restrict__ L
     __syncthreads();
     if (threadIdx.x < kb) dv[threadIdx.x] = T(1) / Cc[threadIdx.x * ldc + K + threadIdx.x];
     __syncthreads();
-    for (int c = warp; c < mc; c += nw) {
-      T v = lane < kb ? Y[(K + lane) * ldy + c] : T(0);
+    for (int cb = warp; cb < mc; cb += nw * kSolveCols) {
+      int col[kSolveCols];
+      bool cv[kSolveCols];
+#pragma unroll
+      for (int q = 0; q < kSolveCols; ++q) {
+        col[q] = cb + q * nw;
+        cv[q] = col[q] < mc;
+        if (!cv[q]) col[q] = cb;
+      }
+      T v[kSolveCols];
+#pragma unroll
+      for (int q = 0; q < kSolveCols; ++q) v[q] = lane < kb ? Y[(K + lane) * ldy + col[q]] : T(0);
       if (lane < kb) {
-        T v2 = T(0);
-        int k = 0;
-        for (; k + 1 < K; k += 2) {
-          v = fma(-Cc[lane * ldc + k], Y[k * ldy + c], v);
-          v2 = fma(-Cc[lane * ldc + k + 1], Y[(k + 1) * ldy + c], v2);
+        for (int k = 0; k < K; ++k) {
+          const T cm = Cc[lane * ldc + k];
+#pragma unroll
+          for (int q = 0; q < kSolveCols; ++q) v[q] = fma(-cm, Y[k * ldy + col[q]], v[q]);
         }
-        if (k < K) v = fma(-Cc[lane * ldc + k], Y[k * ldy + c], v);
-        v += v2;
       }
       for (int j = 0; j < kb; ++j) {
-        const T yj = __shfl_sync(kFull, v, j) * dv[j];
-        if (lane == j) v = yj;
-        else if (lane > j && lane < kb) v = fma(-Cc[lane * ldc + K + j], yj, v);
+        const T cj = (lane > j && lane < kb) ? Cc[lane * ldc + K + j] : T(0);
+#pragma unroll
+        for (int q = 0; q < kSolveCols; ++q) {
+          const T yj = __shfl_sync(kFull, v[q], j) * dv[j];
+          v[q] = lane == j ? yj : fma(-cj, yj, v[q]);
+        }
       }
-      if (lane < kb) Y[(K + lane) * ldy + c] = v;
+      if (lane < kb) {
+#pragma unroll
+        for (int q = 0; q < kSolveCols; ++q)
+          if (cv[q]) Y[(K + lane) * ldy + col[q]] = v[q];
+      }
     }
   }
   __syncthreads();
 }
 
-// Y <- C^{-T} Y (lower C = lower(Lb)), blocks from the bottom, warp per column.
+// Y <- C^{-T} Y (lower C = lower(Lb)), blocks from the bottom, four columns per warp.
 template <typename T>
 __device__ void sweep_upper_solve(T* Y, int ldy, int mc, const T* __restrict__ Lb, int n, T* Cc, T* dv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -686,24 +703,38 @@ __device__ void sweep_upper_solve(T* Y, int ldy, int mc, const T* __restrict__ L
     __syncthreads();
     if (threadIdx.x < kb) dv[threadIdx.x] = T(1) / Cc[threadIdx.x * ldc + threadIdx.x];
     __syncthreads();
-    for (int c = warp; c < mc; c += nw) {
-      T v = lane < kb ? Y[(K + lane) * ldy + c] : T(0);
+    for (int cb = warp; cb < mc; cb += nw * kSolveCols) {
+      int col[kSolveCols];
+      bool cv[kSolveCols];
+#pragma unroll
+      for (int q = 0; q < kSolveCols; ++q) {
+        col[q] = cb + q * nw;
+        cv[q] = col[q] < mc;
+        if (!cv[q]) col[q] = cb;
+      }
+      T v[kSolveCols];
+#pragma unroll
+      for (int q = 0; q < kSolveCols; ++q) v[q] = lane < kb ? Y[(K + lane) * ldy + col[q]] : T(0);
       if (lane < kb) {
-        T v2 = T(0);
-        int k = K + kb;
-        for (; k + 1 < n; k += 2) {
-          v = fma(-Cc[(k - K) * ldc + lane], Y[k * ldy + c], v);
-          v2 = fma(-Cc[(k + 1 - K) * ldc + lane], Y[(k + 1) * ldy + c], v2);
+        for (int k = K + kb; k < n; ++k) {
+          const T cm = Cc[(k - K) * ldc + lane];
+#pragma unroll
+          for (int q = 0; q < kSolveCols; ++q) v[q] = fma(-cm, Y[k * ldy + col[q]], v[q]);
         }
-        if (k < n) v = fma(-Cc[(k - K) * ldc + lane], Y[k * ldy + c], v);
-        v += v2;
       }
       for (int j = kb - 1; j >= 0; --j) {
-        const T xj = __shfl_sync(kFull, v, j) * dv[j];
-        if (lane == j) v = xj;
-        else if (lane < j) v = fma(-Cc[j * ldc + lane], xj, v);
+        const T cj = lane < j ? Cc[j * ldc + lane] : T(0);
+#pragma unroll
+        for (int q = 0; q < kSolveCols; ++q) {
+          const T xj = __shfl_sync(kFull, v[q], j) * dv[j];
+          v[q] = lane == j ? xj : fma(-cj, xj, v[q]);
+        }
       }
-      if (lane < kb) Y[(K + lane) * ldy + c] = v;
+      if (lane < kb) {
+#pragma unroll
+        for (int q = 0; q < kSolveCols; ++q)
+          if (cv[q]) Y[(K + lane) * ldy + col[q]] = v[q];
+      }
     }
   }
   __syncthreads();
