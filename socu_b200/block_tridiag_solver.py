@@ -15,7 +15,6 @@ shape checks (the reference would run them through Warp's CPU backend).
 from __future__ import annotations
 
 import ctypes
-import weakref
 
 import torch
 
@@ -187,11 +186,29 @@ def _settings(block_dim, block_size):
     return out or None
 
 
-def _profiler(lib, h, sh, dev):
+class _LaunchHandle:
+    """Owns one native launch object; destroyed when the last holder (the
+    launch callable and its profile()) goes away."""
+
+    def __init__(self, lib, h, keep=None):
+        self.lib, self.h = lib, h
+        self.keep = keep   # objects the native launch refers to (buffers, a ragged batch)
+
+    def __del__(self):
+        if self.h is not None:
+            self.lib.socu_launch_destroy(self.h)
+            self.h = None
+
+
+def _profiler(lib, handle, sh, dev):
     """profile() of a launch object: device time per kernel kind of one eager
     run (CUDA events around every kernel; synchronises), as
-    {kind: (ms, launches)} for the kinds that ran."""
+    {kind: (ms, launches)} for the kinds that ran.  Holds the handle, so it
+    stays valid even if the launch callable itself is dropped."""
+    h = handle.h
+
     def profile():
+        assert handle.h is not None
         ms = (ctypes.c_double * _lib.KIND_COUNT)()
         cnt = (ctypes.c_int64 * _lib.KIND_COUNT)()
         s = sh if sh is not None else torch.cuda.current_stream(dev).cuda_stream
@@ -268,9 +285,10 @@ def _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, with_x, se
     callback._socu_arrays = keep
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     callback.uses_cuda_graph = bool(use_cuda_graph)
-    callback.profile = _profiler(lib, h, sh, dev)
+    handle = _LaunchHandle(lib, h, keep)
+    callback._handle = handle
+    callback.profile = _profiler(lib, handle, sh, dev)
     callback.settings = dict(settings or {})
-    weakref.finalize(callback, lib.socu_launch_destroy, h)
     return callback
 
 

@@ -779,7 +779,15 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
     if (e != cudaSuccess) return cuda_status(e);
   }
   long long c = 0, cr = 0;
-  int s = enqueue<float>(SOCU_OP_FACTOR_AND_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m), fork);
+  // the float factor of the mixed solve takes its Schur updates on the tcgen05
+  // tensor cores for 64 < n <= 128 unless the tuned table says otherwise: the
+  // 3xTF32 products cost accuracy the FP64 refinement wins back (measured at
+  // N=16384, n=128, m=32: factor 27.0 -> 23.9 ms, still two rounds)
+  socu_tuning mixed{};
+  if (a.n > 64 && update_tc_ok(a.n) && tuning_lookup(SOCU_FLOAT32, a.n, a.m).update_tensor_cores == 0)
+    mixed.update_tensor_cores = 1;
+  int s = enqueue<float>(SOCU_OP_FACTOR_AND_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m), fork,
+                         &mixed);
   if (s != SOCU_OK) return s;
   s = refine_finish_round(a, st, run ? nullptr : &cr);
   if (count) *count = 2 + c + cr;

@@ -303,13 +303,19 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
       const int r0 = rt * 8, ra = r0 + g;
       const bool rv = ra < n;
       const int rr = rv ? ra : 0;
-      double acc[GR][6][2];
+      // accumulators per column group: block (D, E_{i-1}, E_i) x k-step parity
+      // (KP = 2 independent chains per block when there is one group; several
+      // groups already give the MMAs independent chains, and registers are short)
+      constexpr int KP = GR >= 2 ? 1 : 2;
+      double acc[GR][3 * KP][2];
 #pragma unroll
       for (int q = 0; q < GR; ++q)
 #pragma unroll
-        for (int u = 0; u < 6; ++u) acc[q][u][0] = acc[q][u][1] = 0.0;
-#pragma unroll 2
-      for (int k0 = 0; k0 < n; k0 += 8) {
+        for (int u = 0; u < 3 * KP; ++u) acc[q][u][0] = acc[q][u][1] = 0.0;
+      // matrix fragments of one 8-column k-step (two m8n8k4 steps), loaded one
+      // k-step ahead of their products so the global loads overlap the MMAs
+      double fD[2], fM[2], fP[2];
+      auto load_step = [&](int k0) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int k = k0 + 4 * h + t;
@@ -317,9 +323,20 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
           const int kk = kv ? k : 0;
           const bool av = rv && kv;
           const double dv = kk <= rr ? D[rr * n + kk] : D[kk * n + rr];
-          const double aD = av ? dv : 0.0;
-          const double aM = (av && hasM) ? Em[rr * n + kk] : 0.0;
-          const double aP = (av && hasP) ? Ep[kk * n + rr] : 0.0;
+          fD[h] = av ? dv : 0.0;
+          fM[h] = (av && hasM) ? Em[rr * n + kk] : 0.0;
+          fP[h] = (av && hasP) ? Ep[kk * n + rr] : 0.0;
+        }
+      };
+      load_step(0);
+      for (int k0 = 0; k0 < n; k0 += 8) {
+        const double cD[2] = {fD[0], fD[1]}, cM[2] = {fM[0], fM[1]}, cP[2] = {fP[0], fP[1]};
+        if (k0 + 8 < n) load_step(k0 + 8);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k = k0 + 4 * h + t;
+          const bool kv = k < n;
+          const int kk = kv ? k : 0;
 #pragma unroll
           for (int q = 0; q < GR; ++q) {
             if (q >= groups) break;
@@ -327,9 +344,10 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
             const double b1 = kv ? xs0[xstride + xo] : 0.0;
             const double b0 = kv ? xs0[xo] : 0.0;
             const double b2 = kv ? xs0[2 * xstride + xo] : 0.0;
-            dmma_8x8x4(acc[q][h][0], acc[q][h][1], aD, b1);
-            dmma_8x8x4(acc[q][2 + h][0], acc[q][2 + h][1], aM, b0);
-            dmma_8x8x4(acc[q][4 + h][0], acc[q][4 + h][1], aP, b2);
+            const int u = KP == 2 ? h : 0;
+            dmma_8x8x4(acc[q][u][0], acc[q][u][1], cD[h], b1);
+            dmma_8x8x4(acc[q][KP + u][0], acc[q][KP + u][1], cM[h], b0);
+            dmma_8x8x4(acc[q][2 * KP + u][0], acc[q][2 * KP + u][1], cP[h], b2);
           }
         }
       }
@@ -341,8 +359,9 @@ __device__ __forceinline__ void residual_rows_body(const RefineArgs& a, int bi, 
           const int r = r0 + g, c = 8 * q + 2 * t + e;
           if (r < n && c < mc) {
             const long long o = vi + (long long)r * m + c0 + c;
-            const double y = ((acc[q][0][e] + acc[q][1][e]) + (acc[q][2][e] + acc[q][3][e])) +
-                             (acc[q][4][e] + acc[q][5][e]);
+            double y = 0.0;
+#pragma unroll
+            for (int u = 0; u < 3 * KP; ++u) y += acc[q][u][e];
             const double res = a.b[o] - y;
             if (REFINE) {
               a.R32[o] = (float)res;
@@ -374,7 +393,7 @@ __host__ __device__ inline int residual_rows_threads(int n, int) {
 }
 
 template <bool REFINE, int GR>
-__global__ void __launch_bounds__(256, GR == 4 ? 2 : (GR == 2 ? 3 : 4)) k_residual_rows(RefineArgs a) {
+__global__ void __launch_bounds__(256, GR == 4 ? 2 : 3) k_residual_rows(RefineArgs a) {
   pdl_wait();
   pdl_trigger();
   const int bi = blockIdx.x / a.N;

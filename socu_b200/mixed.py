@@ -16,12 +16,11 @@ modified, except x (the solution).
 from __future__ import annotations
 
 import ctypes
-import weakref
 
 import torch
 
 from . import _lib
-from .block_tridiag_solver import _as_tensor, _profiler, _stream_handle, _validate
+from .block_tridiag_solver import _LaunchHandle, _as_tensor, _profiler, _stream_handle, _validate
 
 __all__ = ["create_cholesky_refined_solve_launch", "block_tridiag_residual", "backward_error"]
 
@@ -95,8 +94,9 @@ def create_cholesky_refined_solve_launch(L, E, b, x, mask=None, tol=1e-12, max_i
     # graph mode: the refinement rounds run in a conditional WHILE node
     callback.round_kernel_count = int(lib.socu_launch_round_kernel_count(h))
     # eager run with per-kernel events (all max_iter rounds; not the graph)
-    callback.profile = _profiler(lib, h, sh, dev)
-    weakref.finalize(callback, lib.socu_launch_destroy, h)
+    handle = _LaunchHandle(lib, h, callback._socu_arrays)
+    callback._handle = handle
+    callback.profile = _profiler(lib, handle, sh, dev)
     return callback
 
 

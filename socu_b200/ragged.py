@@ -25,7 +25,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .block_tridiag_solver import _stream_handle
+from .block_tridiag_solver import _LaunchHandle, _profiler, _stream_handle
 
 __all__ = ["RaggedBatch", "ragged_layout", "shard_instances", "create_ragged_factor_and_solve_launch",
            "create_ragged_refined_solve_launch"]
@@ -198,7 +198,9 @@ def _launch(batch, L, E, b, x, tol, eta, iters, stream, use_cuda_graph):
     callback._socu_arrays = (batch, L, E, b, x, eta, iters)
     callback.kernel_count = int(lib.socu_launch_kernel_count(h))
     callback.batch = batch
-    weakref.finalize(callback, lib.socu_launch_destroy, h)
+    handle = _LaunchHandle(lib, h, callback._socu_arrays)
+    callback._handle = handle
+    callback.profile = _profiler(lib, handle, sh, dev)
     return callback
 
 
