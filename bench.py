@@ -49,10 +49,15 @@ RAGGED_COUNT, RAGGED_SEED = 4096, 0
 # profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md
 TRAFFIC_BYTES = 5005218
 TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md"
-# DRAM bytes (read + write) per k_node<float, y, inverse> launch of the mixed
-# solve (ncu capture): none committed yet
-NODE_TRAFFIC_BYTES = None
-NODE_TRAFFIC_NOTE = "no ncu capture of k_node<float> committed"
+# DRAM bytes (read + write) per k_node<float, y, inverse> launch of a float
+# factor_and_solve of this shape, averaged over its 11 levels: ncu capture of
+# `bench.py --ncu-case node` (4 systems, so that the float blocks exceed L2),
+# 254.7 MB over the 11 launches of one pass, per system
+# (profiles/k_node_f32_levels_N1024_n64_m8_B4.md)
+NODE_TRAFFIC_BYTES = 254.66e6 / 4 / 11
+NODE_TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 11 k_node<float,1,1> launches of "
+                     "bench.py --ncu-case node (4 systems, inputs > L2), per system and launch; "
+                     "profiles/k_node_f32_levels_N1024_n64_m8_B4.md")
 RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
                    "instance i seeded with 0 + i, one persistent launch per solve")
 
@@ -527,7 +532,8 @@ def run_ours(args, rank, world, local_rank):
         "phases": dict(budget(phases_mixed), note="one eager run with CUDA events around every kernel, "
                        f"{abs(iters)} rounds; events add gaps, so the sum exceeds ms_per_step"),
         "roofline": {"kernel": f"k_node<float> (level nodes of the mixed solve: potrf + coupling solves + forward "
-                               f"step; largest share of the mixed solve: {dom})",
+                               f"step, averaged over its launches; phase with the largest share of this run's "
+                               f"eager profile: {dom})",
                      "bound": "tensor", "achieved": node_ach, "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": node_ach / bf16_peak, "peak_source": f"{peak_src} (bf16 dense, MEASURED_PEAKS.json)",
                      "traffic": NODE_TRAFFIC_BYTES, "traffic_source": NODE_TRAFFIC_NOTE,
@@ -740,8 +746,9 @@ NCU_CASES = {
 def run_ncu_case(name):
     """Small eager workloads for ncu captures of single kernels (not a bench
     line): two factor_and_solve runs in float and two in FP64 of the case's
-    shape, then one mixed solve without its CUDA graph (ncu does not report
-    kernels inside conditional graph nodes)."""
+    shape, for n > 64 one float factor_and_solve with the tensor-memory node
+    and the tensor-core Schur update, then one mixed solve without its CUDA
+    graph (ncu does not report kernels inside conditional graph nodes)."""
     import torch
 
     from socu_b200.block_tridiag_solver import create_cholesky_factor_and_solve_launch
@@ -755,6 +762,13 @@ def run_ncu_case(name):
             Lw, Ew, xw = L.to(dt), E.to(dt), b.to(dt)
             create_cholesky_factor_and_solve_launch(Lw, Ew, xw, dtype=dt)()
             torch.cuda.synchronize()
+    if c["n"] > 64:
+        # the tensor-memory float node (k_node_tm) with the tensor-core Schur update
+        from socu_b200.block_tridiag_solver import _launch_with_settings
+        Lw, Ew, xw = L.float(), E.float(), b.float()
+        _launch_with_settings("factor_and_solve", Lw, Ew, xw, torch.float32,
+                              {"node_tensor_cores": 4, "update_tensor_cores": 1}, use_cuda_graph=False)()
+        torch.cuda.synchronize()
     x = torch.zeros_like(b)
     run = create_cholesky_refined_solve_launch(L, E, b, x, tol=TOL, max_iter=3, use_cuda_graph=False)
     run()

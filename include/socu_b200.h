@@ -147,7 +147,10 @@ int socu_launch_run(socu_launch_t launch, void* stream);
  * (2, the default: exact products of the float operands, FP64 sums).
  * node_tensor_cores: the coupling and forward products of float level nodes
  * (n <= 128) on the tcgen05 tensor cores at every level (1), only on levels
- * with at least 4 nodes per SM (3), or SIMT (2, and the default). */
+ * with at least 4 nodes per SM (3), or SIMT (2, and the default); 4 keeps a
+ * float level node with 64 < n <= 128 resident in tensor memory and runs the
+ * trailing updates of its blocked Cholesky and coupling solves on the tensor
+ * cores (3xTF32), the 32-column panels on SIMT cores. */
 typedef struct socu_tuning {
   int32_t node_threads;
   int32_t update_threads;

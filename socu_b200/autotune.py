@@ -18,7 +18,9 @@ Settings (``socu_tuning``; 0 = built-in heuristic):
                          tcgen05 tensor cores, 3xTF32 (1), or not (2)
     node_tensor_cores    products of float level nodes (n <= 128) on the
                          tcgen05 tensor cores at every level (1), on wide
-                         levels only (3), or SIMT (2)
+                         levels only (3), or SIMT (2); 64 < n <= 128: the
+                         node resident in tensor memory, trailing updates on
+                         the tensor cores (4)
 
 Search: coordinate descent from the built-in heuristics.  Each knob in turn
 is tried at every value with the others held at the best so far; a candidate
@@ -165,6 +167,8 @@ def candidates(n: int, n_rhs: int, dtype) -> dict:
             continue
         if k == "node_tensor_cores" and (n > 128 or _dtype_name(dtype) == "float64"):
             continue
+        if k == "node_tensor_cores" and n > 64:
+            vals = vals + [4]
         out[k] = vals
     return out
 

@@ -296,12 +296,12 @@ _OPS = {"factor": _lib.OP_FACTOR, "factor_and_solve": _lib.OP_FACTOR_AND_SOLVE, 
         "forward": _lib.OP_FORWARD, "backward": _lib.OP_BACKWARD}
 
 
-def _launch_with_settings(op, L, E, x, dtype, settings, use_cuda_graph=True):
+def _launch_with_settings(op, L, E, x, dtype, settings, use_cuda_graph=True, mask=None, info=None):
     """Graph-captured launch of `op` (a name of _OPS) with explicit launch
     settings (the autotuner's candidates)."""
     with_x = op != "factor"
-    return _create(_OPS[op], L, E, x if with_x else None, None, dtype, None, None, use_cuda_graph, with_x,
-                   settings={k: v for k, v in settings.items() if v})
+    return _create(_OPS[op], L, E, x if with_x else None, mask, dtype, None, None, use_cuda_graph, with_x,
+                   settings={k: v for k, v in settings.items() if v}, info=info)
 
 
 # ---------------------------------------------------------------------------

@@ -1,5 +1,6 @@
 // C ABI of socu_b200: argument validation, level scheduling, kernel enqueue,
 // and launch objects with optional CUDA-graph capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,6 +15,7 @@
 #include "../../include/socu_b200.h"
 #include "grad.cuh"
 #include "ragged.cuh"
+#include "tc_node.cuh"
 #include "tc_update.cuh"
 
 namespace socu {
@@ -186,7 +188,7 @@ bool tuning_valid(const socu_tuning& t) {
   return thr(t.node_threads) && thr(t.update_threads) && thr(t.sweep_threads) && t.sweep_tensor_cores >= 0 &&
          t.sweep_tensor_cores <= 2 && (t.update_tile == 0 || t.update_tile == 16 || t.update_tile == 32) &&
          t.ragged_units >= 0 && t.ragged_units <= 64 && t.update_tensor_cores >= 0 && t.update_tensor_cores <= 2 &&
-         t.node_tensor_cores >= 0 && t.node_tensor_cores <= 3;
+         t.node_tensor_cores >= 0 && t.node_tensor_cores <= 4;
 }
 
 void tuning_merge(socu_tuning* into, const socu_tuning& over) {
@@ -306,6 +308,82 @@ void launch(void (*kernel)(KArgs...), unsigned blocks, unsigned threads, size_t 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// ---------------------------------------------------------------------------
+// TMA tensor maps of the resident sweeps.  cuTensorMapEncodeTiled is a
+// driver-API call; it is resolved through the runtime's entry-point query, so
+// the library does not link against libcuda.  SOCU_TMA=0 keeps the sweeps on
+// per-thread cp.async copies.
+// ---------------------------------------------------------------------------
+using TmaEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TmaEncodeFn tma_encoder() {
+  static const TmaEncodeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || f == nullptr) {
+      (void)cudaGetLastError();
+      return static_cast<TmaEncodeFn>(nullptr);
+    }
+    return reinterpret_cast<TmaEncodeFn>(f);
+  }();
+  return fn;
+}
+
+bool tma_enabled() {
+  static const int on = [] {
+    const char* v = std::getenv("SOCU_TMA");
+    return (v != nullptr && v[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
+// 4-D map {cols, rows, count, batch} of an array of row-major rows x cols
+// tiles (batch entries batch_stride elements apart), box {box_cols, rows, 1, 1}.
+// false when an alignment rule of the TMA unit is not met (the caller then
+// copies with cp.async): base, row, tile and batch strides on 16 bytes, box
+// rows of a multiple of 16 bytes, box extents <= 256.
+bool encode_tiles(CUtensorMap* map, const void* base, int es, int cols, int rows, long long count, int batch,
+                  long long batch_stride, int box_cols) {
+  const TmaEncodeFn enc = tma_encoder();
+  if (enc == nullptr || base == nullptr || cols < 1 || rows < 1 || count < 1 || batch < 1) return false;
+  const unsigned long long row_b = (unsigned long long)cols * es, tile_b = row_b * (unsigned long long)rows;
+  const unsigned long long batch_b =
+      (unsigned long long)(batch > 1 ? batch_stride : count * rows * (long long)cols) * (unsigned long long)es;
+  if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (row_b & 15u) != 0 || (tile_b & 15u) != 0 ||
+      (batch_b & 15u) != 0 || batch_b == 0)
+    return false;
+  if (box_cols < 1 || box_cols > 256 || rows > 256 || ((long long)box_cols * es) % 16 != 0) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)count, (cuuint64_t)batch};
+  const cuuint64_t strides[3] = {row_b, tile_b, batch_b};
+  const cuuint32_t box[4] = {(cuuint32_t)box_cols, (cuuint32_t)rows, 1u, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  return enc(map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+             const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Maps of one op's resident sweeps: factor / coupling blocks with the padded
+// block row (res_ldm), vector chunks with the padded vector row (res_ldy).
+template <typename T>
+SweepMaps sweep_maps(const Problem<T>& p) {
+  SweepMaps m;
+  std::memset(&m, 0, sizeof m);
+  // (the sweeps wait for their block copies in the first vector chunk)
+  if (!tma_enabled() || p.m <= 0 || p.X == nullptr) return m;
+  constexpr int es = sizeof(T);
+  const int ldm = res_ldm(p.n);
+  m.blocks = encode_tiles(&m.L, p.L, es, p.n, p.n, p.N, p.B, p.sL, ldm) &&
+             (p.S == 0 || encode_tiles(&m.E, p.E, es, p.n, p.n, p.S, p.B, p.sE, ldm));
+  m.vecs = p.X != nullptr && p.m > 0 &&
+           encode_tiles(&m.X, p.X, es, p.m, p.n, p.N, p.B, p.sX, res_ldy(std::min(p.m, kMC)));
+  return m;
 }
 
 // The library links the CUDA runtime statically, so its notion of the
@@ -444,6 +522,13 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   const size_t sd_tc = (size_t)smem_node_tc_bytes(n, withY ? p.m : 0);
   auto node_tc_kernel = withY ? (inv ? k_node_tc<true, true> : k_node_tc<true, false>)
                               : (inv ? k_node_tc<false, true> : k_node_tc<false, false>);
+  // float level nodes with 64 < n <= 128 resident in tensor memory, trailing
+  // updates of the blocked factor on the tensor cores (node_tensor_cores = 4)
+  const int m_node = withY ? p.m : 0;
+  const bool node_tm = sizeof(T) == 4 && !inv && cfg.node_tensor_cores == 4 && node_tm_ok(n, m_node) &&
+                       smem_node_tm_bytes(n, m_node) <= (long long)max_smem_optin();
+  const size_t sd_tm = (size_t)smem_node_tm_bytes(n, m_node);
+  auto node_tm_kernel = withY ? k_node_tm<true> : k_node_tm<false>;
   long long launches = 0;
   const bool run = count == nullptr;
   const int sms = run ? sm_count() : 0;
@@ -457,6 +542,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       if (e == cudaSuccess) e = update_uses_big(n) ? prepare(k_update_big<T>, su) : prepare(k_update<T>, su);
       if (e == cudaSuccess && upd_tc) e = prepare(k_update_tc, su_tc);
       if (e == cudaSuccess && node_tc_any) e = prepare(node_tc_kernel, sd_tc);
+      if (e == cudaSuccess && node_tm) e = prepare(node_tm_kernel, sd_tm);
     }
     if (e == cudaSuccess) e = prepare(fwd_kernel, ss);
     if (e == cudaSuccess) e = prepare(pull_kernel, ss);
@@ -481,16 +567,20 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   // first kernel, not the forked branch, not while profiling with events)
   bool first = true;
   auto go_on = [&](cudaStream_t s, auto kernel, int kind, long long blocks, size_t smem, const Level& L,
-                   int threads) {
+                   int threads, auto... extra) {
     if (blocks <= 0) return;
     ++launches;
     if (!run) return;
     const bool pdl = !first && s == st && g_prof == nullptr;
     first = false;
     prof_begin(s, kind);
-    launch(kernel, (unsigned)blocks, (unsigned)threads, smem, s, pdl, p, L);
+    launch(kernel, (unsigned)blocks, (unsigned)threads, smem, s, pdl, p, L, extra...);
     prof_end(s);
   };
+  // TMA maps of the resident sweeps (zeros: cp.async copies)
+  SweepMaps maps;
+  std::memset(&maps, 0, sizeof maps);
+  if (run && res) maps = sweep_maps(p);
   auto node_threads = [&](long long blocks) {
     if (cfg.node_threads) return cfg.node_threads;
     return run ? level_threads(node_kernel, nth, blocks, sd) : nth;
@@ -513,7 +603,9 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       const long long node_blocks = (long long)p.B * L.d;
       if constexpr (sizeof(T) == 4) {
         const bool node_tc = node_tc_any && (!node_tc_wide_only || node_blocks >= 4LL * sms);
-        if (node_tc)
+        if (node_tm)
+          go_on(st, node_tm_kernel, SOCU_KIND_NODE, node_blocks, sd_tm, L, 256);
+        else if (node_tc)
           go_on(st, node_tc_kernel, SOCU_KIND_NODE, node_blocks, sd_tc, L, 256);
         else
           go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
@@ -527,7 +619,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
         if (forked && pull_blocks > 0) {
           cudaEventRecord(fork->split, st);
           cudaStreamWaitEvent(fork->aux, fork->split, 0);
-          go_on(fork->aux, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
+          go_on(fork->aux, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr, maps);
           cudaEventRecord(fork->join, fork->aux);
         }
         const long long upd_blocks = (long long)p.B * update_launch_tasks(n, p.N, L);
@@ -548,21 +640,21 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
           cudaStreamWaitEvent(st, fork->join, 0);
           first = true;   // the next node waits for the forked branch in full
         } else
-          go_on(st, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr);
+          go_on(st, pull_kernel, SOCU_KIND_PULL, pull_blocks, ss, PL, swp_thr, maps);
       }
     }
   }
   if (op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE) {
     for (int l = 0; l < K; ++l) {
       const long long blocks = (long long)p.B * (l == 0 ? lv[l].d : p.N / lv[l].s);
-      go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks, true), swp_thr);
+      go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks, true), swp_thr, maps);
     }
   }
   if (op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE) {
     for (int l = K - 1; l >= 0; --l) {
       const long long blocks = (long long)p.B * lv[l].d;
       go_on(st, bwd_kernel, SOCU_KIND_BACKWARD, blocks, ss,
-            sweep_level(lv[l], blocks, op != SOCU_OP_FACTOR_AND_SOLVE || l != K - 1), swp_thr);
+            sweep_level(lv[l], blocks, op != SOCU_OP_FACTOR_AND_SOLVE || l != K - 1), swp_thr, maps);
     }
   }
   if (count) *count = launches;

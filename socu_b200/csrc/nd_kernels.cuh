@@ -25,6 +25,7 @@
 #pragma once
 
 #include "nd_device.cuh"
+#include "tma.cuh"
 
 namespace socu {
 
@@ -752,9 +753,46 @@ __host__ __device__ inline int res_ldy(int mc) { return ((mc + 3) / 4) * 4 + 4; 
 // 16-byte copy per 4 floats / 2 doubles) and 4 threads x 8 rows of a warp hit
 // distinct banks in the row-major reads
 __host__ __device__ inline int res_ldm(int n) { return ((n + 3) & ~3) + 4; }
+// elements of one resident-sweep region, rounded so the next region starts on
+// 128 bytes (TMA destinations)
+__host__ __device__ inline long long res_round(long long elems, int es) {
+  const long long q = 128 / es;
+  return ((elems + q - 1) / q) * q;
+}
+// three vector regions, three block regions, dv (n) and two mbarriers; the
+// 4-byte rounding is the larger, so the count covers both element sizes
 __host__ __device__ inline long long smem_sweep_res_elems(int n, int m) {
   const int mc = min_i(m, kMC);
-  return 3LL * n * res_ldm(n) + 3LL * n * res_ldy(mc) + n;
+  return 3LL * res_round((long long)n * res_ldy(mc), 4) + 3LL * res_round((long long)n * res_ldm(n), 4) + n + 8;
+}
+
+// TMA use of one resident-sweep CTA: block and vector loads by the validity of
+// their maps and a 128-byte aligned shared base (the same in every thread);
+// initialises the two mbarriers (all threads call).
+struct ResTma {
+  bool blocks, vecs;
+};
+__device__ __forceinline__ ResTma res_tma_begin(const SweepMaps* tm, unsigned char* raw, uint64_t* bar) {
+  ResTma r{false, false};
+  if (tm == nullptr || (smem_addr(raw) & 127u) != 0) return r;
+  r.blocks = tm->blocks != 0;
+  r.vecs = tm->vecs != 0;
+  if (r.blocks || r.vecs) {
+    if (threadIdx.x == 0) {
+      tc::mbar_init(bar, 1);
+      tc::mbar_init(bar + 1, 1);
+    }
+    __syncthreads();
+  }
+  return r;
+}
+
+// Wait for this chunk's TMA copies: the blocks (first chunk) and the vectors;
+// false (in every thread) if a wait ran out.
+__device__ __forceinline__ bool res_tma_wait(const ResTma& tu, bool blocks_pending, uint64_t* bar, int chunk) {
+  const bool okb = (tu.blocks && blocks_pending) ? tma::wait(bar, 0) : true;
+  const bool okv = tu.vecs ? tma::wait(bar + 1, (unsigned)chunk & 1u) : true;
+  return okb && okv;
 }
 
 // CW consecutive elements from 16-byte-aligned shared memory (8-byte for CW = 2 floats)
@@ -1060,10 +1098,10 @@ __host__ __device__ inline int fwd_tasks(int N, const Level& lv) { return lv.s =
 
 template <typename T, bool RES, bool PULL_ONLY, bool INV>
 __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, int b, int task,
-                                         unsigned char* smem_raw) {
+                                         unsigned char* smem_raw, const SweepMaps* tm = nullptr) {
   const int s = lv.s, N = p.N, n = p.n;
   const int h = s / 2;
-  int j;
+  int j, slot = 0;
   bool pull, solve;
   const T *F = nullptr, *G = nullptr;
   if (s == 1) {
@@ -1075,36 +1113,64 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
     j = s * u - 1;
     pull = true;
     solve = !PULL_ONLY && (u & 1) != 0;
-    F = p.Eb(b, lv.op + 2 * u - 2);
-    if (j + h < N) G = p.Eb(b, lv.op + 2 * u - 1);
+    slot = lv.op + 2 * u - 2;
+    F = p.Eb(b, slot);
+    if (j + h < N) G = p.Eb(b, slot + 1);
   }
   const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : sweep_ldy(mcmax);
+  // RES: Y, Z1, Z2 (n x ldy), C, F, G (n x ldm), dv (n), two mbarriers, regions on
+  // 128 bytes; else Y, Z1, Z2, Cc (smem_sweep_elems), dv
+  const long long vy = RES ? res_round((long long)n * ldy, sizeof(T)) : (long long)n * ldy;
   T* Y = reinterpret_cast<T*>(smem_raw);
-  T* Z1 = Y + n * ldy;
-  T* Z2 = Z1 + n * ldy;
-  T* Ms = Z2 + n * ldy;   // RES: C, F, G (n x ldm each), dv (n); else Cc (smem_sweep_elems), dv
+  T* Z1 = Y + vy;
+  T* Z2 = Z1 + vy;
+  T* Ms = Z2 + vy;
   const int ldm = res_ldm(n);
+  const long long vm = res_round((long long)n * ldm, sizeof(T));
   T* Cs = Ms;
-  T* Fs = Cs + n * ldm;
-  T* Gs = Fs + n * ldm;
-  T* dv = RES ? Gs + n * ldm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
+  T* Fs = Cs + vm;
+  T* Gs = Fs + vm;
+  T* dv = RES ? Gs + vm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((reinterpret_cast<unsigned char*>(dv + n) - smem_raw + 7) & ~7LL));
   T* yj = p.Xb(b, j);
   const T* Lj = p.Lb(b, j);
+  const ResTma tu = RES ? res_tma_begin(tm, smem_raw, bar) : ResTma{false, false};
+  const int nblk = RES ? (solve ? 1 : 0) + (F ? 1 : 0) + (G ? 1 : 0) : 0;
   if (!lv.pre) pdl_wait();
   if (RES) {
-    if (solve) async_load(Cs, ldm, Lj, n, n, n);
-    if (F) async_load(Fs, ldm, F, n, n, n);
-    if (G) async_load(Gs, ldm, G, n, n, n);
+    if (tu.blocks) {
+      if (threadIdx.x == 0 && nblk > 0) {
+        tma::expect_tx(bar, (uint32_t)(nblk * n * ldm * sizeof(T)));
+        if (solve) tma::load_4d(Cs, &tm->L, 0, 0, j, b, bar);
+        if (F) tma::load_4d(Fs, &tm->E, 0, 0, slot, b, bar);
+        if (G) tma::load_4d(Gs, &tm->E, 0, 0, slot + 1, b, bar);
+      }
+    } else {
+      if (solve) async_load(Cs, ldm, Lj, n, n, n);
+      if (F) async_load(Fs, ldm, F, n, n, n);
+      if (G) async_load(Gs, ldm, G, n, n, n);
+    }
   }
   if (lv.pre) pdl_wait();
   pdl_trigger();
-  for (int c0 = 0; c0 < p.m; c0 += kMC) {
+  for (int c0 = 0, chunk = 0; c0 < p.m; c0 += kMC, ++chunk) {
     const int mc = min_i(kMC, p.m - c0);
     __syncthreads();
-    async_load(Y, ldy, yj + c0, n, mc, p.m);
-    if (pull) async_load(Z1, ldy, p.Xb(b, j - h) + c0, n, mc, p.m);
-    if (G) async_load(Z2, ldy, p.Xb(b, j + h) + c0, n, mc, p.m);
+    if (tu.vecs) {
+      if (threadIdx.x == 0) {
+        tma::fence_proxy();
+        tma::expect_tx(bar + 1, (uint32_t)((1 + (pull ? 1 : 0) + (G ? 1 : 0)) * n * ldy * sizeof(T)));
+        tma::load_4d(Y, &tm->X, c0, 0, j, b, bar + 1);
+        if (pull) tma::load_4d(Z1, &tm->X, c0, 0, j - h, b, bar + 1);
+        if (G) tma::load_4d(Z2, &tm->X, c0, 0, j + h, b, bar + 1);
+      }
+    } else {
+      async_load(Y, ldy, yj + c0, n, mc, p.m);
+      if (pull) async_load(Z1, ldy, p.Xb(b, j - h) + c0, n, mc, p.m);
+      if (G) async_load(Z2, ldy, p.Xb(b, j + h) + c0, n, mc, p.m);
+    }
     cp_async_wait_all();
+    if ((tu.blocks || tu.vecs) && !res_tma_wait(tu, nblk > 0 && chunk == 0, bar, chunk)) return;
     __syncthreads();
     if (RES) {
       if (c0 == 0 && solve)
@@ -1139,13 +1205,13 @@ __device__ __forceinline__ void fwd_body(const Problem<T>& p, const Level& lv, i
 }
 
 template <typename T, bool RES, bool PULL_ONLY = false, bool INV = false>
-__global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
+__global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv, const __grid_constant__ SweepMaps tm) {
   const int per_b = fwd_tasks(p.N, lv);
   const int b = blockIdx.x / per_b;
   const int task = blockIdx.x - b * per_b;
   if (!p.active(b)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  fwd_body<T, RES, PULL_ONLY, INV>(p, lv, b, task, smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  fwd_body<T, RES, PULL_ONLY, INV>(p, lv, b, task, smem_raw, &tm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1153,39 +1219,65 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv) {
 // ---------------------------------------------------------------------------
 template <typename T, bool RES, bool INV>
 __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, int b, int t,
-                                         unsigned char* smem_raw) {
+                                         unsigned char* smem_raw, const SweepMaps* tm = nullptr) {
   const int n = p.n, s = lv.s, N = p.N;
   const int i = s - 1 + 2 * s * t;
   const int mcmax = min_i(p.m, kMC), ldy = RES ? res_ldy(mcmax) : sweep_ldy(mcmax);
+  // shared layout as in fwd_body
+  const long long vy = RES ? res_round((long long)n * ldy, sizeof(T)) : (long long)n * ldy;
   T* Y = reinterpret_cast<T*>(smem_raw);
-  T* Z1 = Y + n * ldy;
-  T* Z2 = Z1 + n * ldy;
-  T* Ms = Z2 + n * ldy;
+  T* Z1 = Y + vy;
+  T* Z2 = Z1 + vy;
+  T* Ms = Z2 + vy;
   const int ldm = res_ldm(n);
+  const long long vm = res_round((long long)n * ldm, sizeof(T));
   T* Cs = Ms;
-  T* Fs = Cs + n * ldm;
-  T* Gs = Fs + n * ldm;
-  T* dv = RES ? Gs + n * ldm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
+  T* Fs = Cs + vm;
+  T* Gs = Fs + vm;
+  T* dv = RES ? Gs + vm : Ms + (smem_sweep_elems(n, p.m) - 3LL * n * ldy - kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((reinterpret_cast<unsigned char*>(dv + n) - smem_raw + 7) & ~7LL));
   const bool right = i + s < N, left = i >= s;
-  const T* F = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
-  const T* G = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
+  const int slot = lv.oc + 2 * t;
+  const T* F = right ? p.Eb(b, slot) : nullptr;
+  const T* G = left ? p.Eb(b, slot - 1) : nullptr;
   const T* Li = p.Lb(b, i);
   T* xi = p.Xb(b, i);
+  const ResTma tu = RES ? res_tma_begin(tm, smem_raw, bar) : ResTma{false, false};
   if (!lv.pre) pdl_wait();
   if (RES) {
-    async_load(Cs, ldm, Li, n, n, n);
-    if (right) async_load(Fs, ldm, F, n, n, n);
-    if (left) async_load(Gs, ldm, G, n, n, n);
+    if (tu.blocks) {
+      if (threadIdx.x == 0) {
+        tma::expect_tx(bar, (uint32_t)((1 + (right ? 1 : 0) + (left ? 1 : 0)) * n * ldm * sizeof(T)));
+        tma::load_4d(Cs, &tm->L, 0, 0, i, b, bar);
+        if (right) tma::load_4d(Fs, &tm->E, 0, 0, slot, b, bar);
+        if (left) tma::load_4d(Gs, &tm->E, 0, 0, slot - 1, b, bar);
+      }
+    } else {
+      async_load(Cs, ldm, Li, n, n, n);
+      if (right) async_load(Fs, ldm, F, n, n, n);
+      if (left) async_load(Gs, ldm, G, n, n, n);
+    }
   }
   if (lv.pre) pdl_wait();
   pdl_trigger();
-  for (int c0 = 0; c0 < p.m; c0 += kMC) {
+  for (int c0 = 0, chunk = 0; c0 < p.m; c0 += kMC, ++chunk) {
     const int mc = min_i(kMC, p.m - c0);
     __syncthreads();
-    async_load(Y, ldy, xi + c0, n, mc, p.m);
-    if (right) async_load(Z1, ldy, p.Xb(b, i + s) + c0, n, mc, p.m);
-    if (left) async_load(Z2, ldy, p.Xb(b, i - s) + c0, n, mc, p.m);
+    if (tu.vecs) {
+      if (threadIdx.x == 0) {
+        tma::fence_proxy();
+        tma::expect_tx(bar + 1, (uint32_t)((1 + (right ? 1 : 0) + (left ? 1 : 0)) * n * ldy * sizeof(T)));
+        tma::load_4d(Y, &tm->X, c0, 0, i, b, bar + 1);
+        if (right) tma::load_4d(Z1, &tm->X, c0, 0, i + s, b, bar + 1);
+        if (left) tma::load_4d(Z2, &tm->X, c0, 0, i - s, b, bar + 1);
+      }
+    } else {
+      async_load(Y, ldy, xi + c0, n, mc, p.m);
+      if (right) async_load(Z1, ldy, p.Xb(b, i + s) + c0, n, mc, p.m);
+      if (left) async_load(Z2, ldy, p.Xb(b, i - s) + c0, n, mc, p.m);
+    }
     cp_async_wait_all();
+    if ((tu.blocks || tu.vecs) && !res_tma_wait(tu, chunk == 0, bar, chunk)) return;
     __syncthreads();
     if (RES) {
       if (c0 == 0)
@@ -1220,12 +1312,12 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
 }
 
 template <typename T, bool RES, bool INV = false>
-__global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv) {
+__global__ void __launch_bounds__(256) k_bwd(Problem<T> p, Level lv, const __grid_constant__ SweepMaps tm) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
   if (!p.active(b)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  bwd_body<T, RES, INV>(p, lv, b, t, smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  bwd_body<T, RES, INV>(p, lv, b, t, smem_raw, &tm);
 }
 
 }  // namespace socu

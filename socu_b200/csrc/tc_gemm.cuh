@@ -32,6 +32,10 @@ __device__ __forceinline__ uint32_t saddr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// Error word of the asynchronous units on one device: 1 a tensor-core wait
+// ran out, 2 a TMA copy wait ran out (that kernel skipped its result).
+__device__ int g_tc_error;
+
 // ---- instruction / shared-memory descriptors --------------------------------
 // kind::tf32 instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32
 // (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
@@ -137,6 +141,17 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
+// warp-wide: 32 lanes x 8 consecutive 32-bit columns from registers; thread t writes lane (taddr lane + t)
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(taddr),
+               "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+               "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+               "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+
 // ---- TF32 split --------------------------------------------------------------
 // round-to-nearest TF32 (10 explicit mantissa bits) of an FP32 value; the
 // remainder a - hi is exact in FP32
@@ -146,12 +161,16 @@ __device__ __forceinline__ float tf32_hi(float a) {
   return __uint_as_float(r);
 }
 
-// Store value v of operand element (m, k) into the hi / lo planes.
+// Store value v of operand element (m, k) into the hi / lo planes.  The
+// remainder is rounded to TF32 as well (the tensor core would otherwise drop
+// its low 13 mantissa bits, a truncation): each of the two pieces is then
+// within half a TF32 unit, and a product of split operands misses only
+// ~2^-23 of |a b| -- the FP32 rounding level.
 __device__ __forceinline__ void put_split(unsigned char* hi, unsigned char* lo, int m, int k, int K, float v) {
   const uint32_t o = coff(m, k, K);
   const float h = tf32_hi(v);
   *reinterpret_cast<float*>(hi + o) = h;
-  *reinterpret_cast<float*>(lo + o) = v - h;
+  *reinterpret_cast<float*>(lo + o) = tf32_hi(v - h);
 }
 
 // One thread: the 3xTF32 MMAs of D (M x N) (+)= A * B^T over K (multiple of

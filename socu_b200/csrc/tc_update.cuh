@@ -36,8 +36,7 @@ __host__ __device__ inline long long smem_update_tc_bytes(int n) {
 }
 __host__ __device__ inline bool update_tc_ok(int n) { return n >= 1 && n <= kTcMaxN; }
 
-// Error word of the tensor-core kernels (1: a wait ran out); one per device.
-__device__ int g_tc_error;
+using tc::g_tc_error;
 
 // Stage columns [k0, k0 + KC) of a rows x K operand into hi/lo planes of a
 // KC-column chunk.  val(r, k) gives the element (only called for r < rows,
@@ -63,8 +62,41 @@ __device__ __forceinline__ void tc_stage(unsigned char* hi, unsigned char* lo, i
   tc_stage_kc<kTcKC>(hi, lo, rows_pad, rows, K, k0, val);
 }
 
-// One update task (see the file comment), all threads of the CTA (multiple
-// of 128).  tmem: 128-column accumulator of this CTA; bar: its mbarrier,
+// The same staging in two halves, so that a chunk's global loads can be
+// issued while the previous chunk's MMAs run: tc_load_kc reads this thread's
+// elements (unit order of tc_stage_kc, at most MAXU per thread) into
+// registers, tc_put_kc splits them into the planes.
+template <int KC, int MAXU, class Val>
+__device__ __forceinline__ void tc_load_kc(float (&v)[MAXU], int rows_pad, int rows, int K, int k0, Val val) {
+  constexpr int kq = KC / 4;
+  const int units = (rows_pad / 8) * kq;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < MAXU; ++j) {
+    const int u = warp + j * nw;
+    const int r = (u / kq) * 8 + (lane >> 2);
+    const int k = k0 + (u % kq) * 4 + (lane & 3);
+    v[j] = (u < units && r < rows && k < K) ? val(r, k) : 0.0f;
+  }
+}
+
+template <int KC, int MAXU>
+__device__ __forceinline__ void tc_put_kc(unsigned char* hi, unsigned char* lo, const float (&v)[MAXU],
+                                          int rows_pad) {
+  constexpr int kq = KC / 4;
+  const int units = (rows_pad / 8) * kq;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < MAXU; ++j) {
+    const int u = warp + j * nw;
+    if (u < units) tc::put_split(hi, lo, (u / kq) * 8 + (lane >> 2), (u % kq) * 4 + (lane & 3), KC, v[j]);
+  }
+}
+// per-thread elements of a 128 x kTcKC chunk at 256 threads
+constexpr int kTcUnitsPerThread = 128 / 8 * (kTcKC / 4) / 8;
+
+// One update task (see the file comment), all 256 threads of the CTA (the
+// register staging holds kTcUnitsPerThread elements per thread at 256).  tmem: 128-column accumulator of this CTA; bar: its mbarrier,
 // phase counter in *phase (the caller keeps it across tasks).
 __device__ __forceinline__ void update_tc_body(const Problem<float>& p, const Level& lv, int b, int task,
                                                unsigned char* smem, uint32_t tmem, uint64_t* bar,
@@ -95,13 +127,37 @@ __device__ __forceinline__ void update_tc_body(const Problem<float>& p, const Le
     K = n;
   }
   bool ok;
+  // A = [F | G^T] (target) or F (fill-in): A(r, k) = k < n ? F[r][k] : G[k-n][r];
+  // fill-in: B(c, k) = G[k][c]; targets use B = A (its first nc rows).  The
+  // next chunk's elements are loaded into registers while this chunk's MMAs run.
+  // With 8 warps and 8 four-column groups per chunk, a thread's elements
+  // (tc_put_kc's unit order) are one column k0 + kk of the chunk at rows
+  // lane / 4 + 8 j: a strided run in F (rows) or G (columns).
+  float ra[kTcUnitsPerThread], rb[kTcUnitsPerThread];
+  const int kk = (threadIdx.x >> 5) * 4 + (threadIdx.x & 3), r0 = (threadIdx.x & 31) >> 2;
+  auto load_chunk = [&](int k0) {
+    const int k = k0 + kk;
+    const float* a = nullptr;
+    long long sa = 0;
+    if (k < n) {
+      a = F + (long long)r0 * n + k;
+      sa = 8LL * n;
+    } else if (k < K) {
+      a = G + (long long)(k - n) * n + r0;
+      sa = 8;
+    }
+#pragma unroll
+    for (int j = 0; j < kTcUnitsPerThread; ++j) ra[j] = (a != nullptr && r0 + 8 * j < n) ? a[j * sa] : 0.0f;
+    if (!target) {
+      const float* g = k < K ? G + (long long)k * n + r0 : nullptr;
+#pragma unroll
+      for (int j = 0; j < kTcUnitsPerThread; ++j) rb[j] = (g != nullptr && r0 + 8 * j < n) ? g[8 * j] : 0.0f;
+    }
+  };
+  load_chunk(0);
   for (int k0 = 0; k0 < K; k0 += kTcKC) {
-    // A = [F | G^T] (target) or F (fill-in): A(r, k) = k < n ? F[r][k] : G[k-n][r]
-    tc_stage(a_hi, a_lo, 128, n, K, k0, [&](int r, int k) {
-      return k < n ? F[(long long)r * n + k] : G[(long long)(k - n) * n + r];
-    });
-    // fill-in: B(c, k) = G[k][c]; targets use B = A (its first nc rows)
-    if (!target) tc_stage(b_hi, b_lo, nc, n, K, k0, [&](int c, int k) { return G[(long long)k * n + c]; });
+    tc_put_kc<kTcKC, kTcUnitsPerThread>(a_hi, a_lo, ra, 128);
+    if (!target) tc_put_kc<kTcKC, kTcUnitsPerThread>(b_hi, b_lo, rb, nc);
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -112,6 +168,7 @@ __device__ __forceinline__ void update_tc_body(const Problem<float>& p, const Le
       tc::gemm_3xtf32(tmem, ah, al, bh, bl, nc, kTcKC, k0 > 0 ? 1u : 0u);
       tc::commit(bar);
     }
+    if (k0 + kTcKC < K) load_chunk(k0 + kTcKC);
     // every thread waits for the chunk's MMAs before the buffer is restaged;
     // the vote keeps the CTA's control flow uniform if a wait runs out
     const bool done = tc::mbar_wait(bar, *phase & 1u, kTcWaitNs);
@@ -149,7 +206,7 @@ __device__ __forceinline__ void update_tc_body(const Problem<float>& p, const Le
 }
 
 // One CTA per update task of one level (grid = B x update_blocks).
-__global__ void __launch_bounds__(256, 1) k_update_tc(Problem<float> p, Level lv) {
+__global__ void __launch_bounds__(256, 3) k_update_tc(Problem<float> p, Level lv) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tbase;

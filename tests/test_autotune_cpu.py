@@ -41,7 +41,7 @@ def test_table_exact_and_wildcard_entries():
 
 @pytest.mark.parametrize("bad", [{"node_threads": 96}, {"update_tile": 8}, {"sweep_tensor_cores": 3},
                                  {"ragged_units": 65}, {"sweep_threads": 512}, {"update_tensor_cores": 3},
-                                 {"node_tensor_cores": 4}])
+                                 {"node_tensor_cores": 5}])
 def test_table_rejects_invalid_settings(bad):
     with pytest.raises(RuntimeError):
         autotune.install(torch.float64, 16, 1, bad)

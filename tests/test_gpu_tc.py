@@ -113,8 +113,9 @@ def test_tc_node_parity(n, m, op):
         assert rel < 1e-4, (settings, rel)
 
 
-@pytest.mark.parametrize("n,m", [(32, 4), (64, 8), (128, 8)])
-def test_refined_solve_with_tensor_cores(n, m):
+@pytest.mark.parametrize("node_tc", [1, 4])
+@pytest.mark.parametrize("n,m", [(32, 4), (64, 8), (128, 8), (96, 32)])
+def test_refined_solve_with_tensor_cores(n, m, node_tc):
     """The mixed solve's float factor on the tensor cores (tuned table entry)
     still reaches the FP64 backward-error bound."""
     import numpy as np
@@ -126,7 +127,7 @@ def test_refined_solve_with_tensor_cores(n, m):
     N = 64
     L_np, E_np, b_np = generators.readme_problem(N, n, m, shift=10.0 + 2.0 * np.sqrt(n), seed=3)
     L, E, b = (torch.tensor(a, device="cuda") for a in (L_np, E_np, b_np))
-    autotune.install(torch.float32, n, m, {"node_tensor_cores": 1, "update_tensor_cores": 1})
+    autotune.install(torch.float32, n, m, {"node_tensor_cores": node_tc, "update_tensor_cores": 1})
     try:
         x = torch.zeros_like(b)
         run = create_cholesky_refined_solve_launch(L, E, b, x, tol=1e-12, max_iter=10)
@@ -136,3 +137,64 @@ def test_refined_solve_with_tensor_cores(n, m):
         autotune.install(torch.float32, n, m, None)
     assert float(run.eta.max()) <= 1e-12, (float(run.eta.max()), int(run.iterations.max()))
     assert nd.backward_error(L_np, E_np, x.cpu().numpy(), b_np)[0] <= 1e-12
+
+
+@pytest.mark.parametrize("n,m", [(72, 1), (96, 5), (100, 3), (128, 32), (128, 1), (120, 64)])
+@pytest.mark.parametrize("op", ["factor_and_solve", "factor+solve"])
+def test_tmem_node_parity(n, m, op):
+    """Float level nodes with 64 < n <= 128 resident in tensor memory, trailing
+    updates on the tensor cores (node_tensor_cores=4), alone and with the
+    tensor-core Schur update: solution and factor layout against the oracle."""
+    import ctypes
+
+    import numpy as np
+
+    from oracle import generators, nd_cholesky as nd
+    from socu_b200.block_tridiag_solver import _launch_with_settings
+
+    N = 37
+    L_np, E_np, b_np = generators.readme_problem(N, n, m, shift=10.0 + 2.0 * np.sqrt(n), seed=200 + n)
+    Lf_ref, Ef_ref, x_ref = nd.nd_factor_and_solve(L_np, E_np, b_np)
+    lib = _lib.load()
+    for settings in ({"node_tensor_cores": 4}, {"node_tensor_cores": 4, "update_tensor_cores": 1}):
+        L, E, x = (torch.tensor(a, dtype=torch.float32, device="cuda") for a in (L_np, E_np, b_np))
+        if op == "factor_and_solve":
+            _launch_with_settings("factor_and_solve", L, E, x, torch.float32, settings)()
+        else:
+            _launch_with_settings("factor", L, E, None, torch.float32, settings)()
+            torch.cuda.synchronize()
+            # factor layout: lower(L_i) = C_i with a zero upper triangle, E as the oracle's
+            Lh = L.double().cpu().numpy()
+            assert np.array_equal(np.triu(Lh, 1), np.zeros_like(Lh))
+            assert np.abs(Lh - Lf_ref[0]).max() <= 1e-4 * np.abs(Lf_ref).max()
+            assert np.abs(E.double().cpu().numpy() - Ef_ref[0]).max() <= 1e-4 * max(1.0, np.abs(Ef_ref).max())
+            _launch_with_settings("solve", L, E, x, torch.float32, settings)()
+        torch.cuda.synchronize()
+        flag = ctypes.c_int(0)
+        assert lib.socu_tc_error(ctypes.byref(flag), 1) == 0 and flag.value == 0
+        rel = np.abs(x.double().cpu().numpy() - x_ref[0]).max() / np.abs(x_ref).max()
+        assert rel < 1e-4, (settings, rel)
+
+
+@pytest.mark.parametrize("use_cuda_graph", [False, True])
+def test_tmem_node_info_and_mask(use_cuda_graph):
+    """node_tensor_cores=4 reports the first failing node (here a negated level-0
+    block, node 6) and leaves masked-out instances untouched."""
+    import numpy as np
+
+    from oracle import generators
+    from socu_b200.block_tridiag_solver import _launch_with_settings
+
+    N, n, m = 20, 96, 3
+    P = [generators.readme_problem(N, n, m, shift=30.0, seed=60 + k) for k in range(3)]
+    L0, E0, b0 = (np.stack([q[i] for q in P]) for i in range(3))
+    L0[1][6] = -L0[1][6]
+    L, E, x = (torch.tensor(a, dtype=torch.float32, device="cuda") for a in (L0, E0, b0))
+    mask = torch.tensor([1, 1, 0], dtype=torch.bool, device="cuda")
+    info = torch.full((3,), -7, dtype=torch.int32, device="cuda")
+    _launch_with_settings("factor_and_solve", L, E, x, torch.float32, {"node_tensor_cores": 4}, mask=mask,
+                          info=info, use_cuda_graph=use_cuda_graph)()
+    torch.cuda.synchronize()
+    assert info.tolist() == [0, 7, 0]
+    assert torch.isfinite(x[0]).all()
+    assert torch.equal(x[2].cpu(), torch.tensor(b0[2], dtype=torch.float32))
