@@ -603,12 +603,27 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
       const long long node_blocks = (long long)p.B * L.d;
       if constexpr (sizeof(T) == 4) {
         const bool node_tc = node_tc_any && (!node_tc_wide_only || node_blocks >= 4LL * sms);
+        // inverse-first nodes on levels that fit one wave of CTAs with the W^T
+        // buffer: the chain also writes W^T and the products run from it
+        auto node_wt_kernel = withY ? (inv ? k_node<float, true, true, true> : k_node<float, true, false, true>)
+                                    : (inv ? k_node<float, false, true, true> : k_node<float, false, false, true>);
+        const size_t sd_wt = (size_t)smem_node_gemm_elems(n, withY ? p.m : 0, 4, true) * 4;
+        const int nthr = node_threads(node_blocks);
+        bool node_wt = false;
+        if (run && !node_tm && !node_tc && node_uses_gemm(n) && reg_chain_ok(n, nthr) &&
+            sd_wt <= (size_t)max_smem_optin() && sms > 0 && prepare(node_wt_kernel, sd_wt) == cudaSuccess) {
+          int dev = 0;
+          cudaGetDevice(&dev);
+          node_wt = (long long)occupancy(node_wt_kernel, dev, nthr, sd_wt) * sms >= node_blocks;
+        }
         if (node_tm)
           go_on(st, node_tm_kernel, SOCU_KIND_NODE, node_blocks, sd_tm, L, 256);
         else if (node_tc)
           go_on(st, node_tc_kernel, SOCU_KIND_NODE, node_blocks, sd_tc, L, 256);
+        else if (node_wt)
+          go_on(st, node_wt_kernel, SOCU_KIND_NODE, node_blocks, sd_wt, L, nthr);
         else
-          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
+          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, nthr);
       } else {
         go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
       }

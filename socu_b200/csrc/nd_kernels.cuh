@@ -149,6 +149,256 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
 }
 
 // ---------------------------------------------------------------------------
+// Float blocked Cholesky against the identity (cta_chol_solve<float, true,
+// true>: lower(A) = C, V = C^{-1}) with the trailing matrices held in
+// registers.  Each thread owns one fixed 4x4 tile for the whole
+// factorisation -- a lower tile of A right of the first panel, or a strictly
+// lower tile of V below the first rows (the only tiles a rank update ever
+// touches) -- instead of loading and storing accumulators around each
+// 8-column step's rank-8 update; a tile goes back to shared memory when it
+// enters the next step's panel (A: its columns, V: its rows).  The item
+// solves also write the solved panel transposed (Pt[k][row]) and the solved
+// rows of V (Vt[k][col]), so both operands of the update are 16-byte loads.
+// Same operations in the same order as cta_chol_solve: identical results.
+// Returns false (nothing done) when the tiles outnumber the threads.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int reg_chain_ldt(int n) { return ((n + 3) / 4) * 4 + 4; }
+// tiles the rank updates touch: A (row block >= column block >= 2), V (row block > column block, row block >= 2)
+__host__ __device__ inline int reg_chain_tiles_a(int n) { const int b = (n + 3) / 4; return b < 3 ? 0 : (b - 2) * (b - 1) / 2; }
+__host__ __device__ inline int reg_chain_tiles_v(int n) { const int b = (n + 3) / 4; return b < 3 ? 0 : (b - 1) * b / 2 - 1; }
+__host__ __device__ inline bool reg_chain_ok(int n, int threads) {
+  return n <= 64 && reg_chain_tiles_a(n) + reg_chain_tiles_v(n) <= threads;
+}
+
+// WT (optional, n x reg_chain_ldt(n), zero on entry): receives W^T, WT[c][r] = V[r][c],
+// from the item solves (every final entry of V comes out of one).
+__device__ bool cta_chol_inv_regs(float* A, int lda, int n, float* V, int ldv, float* Pt, float* Vt,
+                                  float* WT = nullptr) {
+  constexpr int BK = 8;
+  const int na = reg_chain_tiles_a(n), total = na + reg_chain_tiles_v(n);
+  if (total > (int)blockDim.x) return false;
+  const int ldt = reg_chain_ldt(n);
+  // this thread's tile
+  const int id = threadIdx.x;
+  const bool own = id < total, isA = id < na;
+  int r0 = 0, c0 = 0;
+  if (own) {
+    if (isA) {
+      int a = 0;
+      while ((a + 1) * (a + 2) / 2 <= id) ++a;
+      r0 = 4 * (2 + a);
+      c0 = 4 * (2 + id - a * (a + 1) / 2);
+    } else {
+      const int v = id - na;
+      int rb = 2;
+      while ((rb + 1) * rb / 2 - 1 <= v) ++rb;   // tiles before row block rb + 1
+      r0 = 4 * rb;
+      c0 = 4 * (v - ((rb - 1) * rb / 2 - 1));
+    }
+  }
+  float acc[4][4];
+  {
+    const float* src = isA ? A : V;
+    const int ld = isA ? lda : ldv;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = r0 + i, c = c0 + j;
+        acc[i][j] = (own && r < n && c < n) ? src[r * ld + c] : 0.0f;
+      }
+  }
+  for (int K = 0; K < n; K += BK) {
+    const int kb = min(BK, n - K);
+    const int R0 = K + kb, rows = n - R0;
+    const int nv = min(n, R0);
+    // 1.-2. diagonal block in registers and item solves (as cta_chol_solve),
+    //       the solved values also into Pt / Vt
+    float c[BK][BK], rsv[BK];
+    const bool act = threadIdx.x < max(rows + nv, 1);
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < BK; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) c[i][j] = (i < kb) ? A[(K + i) * lda + K + j] : (i == j ? 1.0f : 0.0f);
+#pragma unroll
+      for (int j = 0; j < BK; ++j) {
+        const float r = rsqrt_t(c[j][j]);
+        rsv[j] = r;
+        c[j][j] *= r;
+#pragma unroll
+        for (int i = j + 1; i < BK; ++i) c[i][j] *= r;
+#pragma unroll
+        for (int i = j + 1; i < BK; ++i)
+#pragma unroll
+          for (int l = j + 1; l <= i; ++l) c[i][l] = fma(-c[i][j], c[l][j], c[i][l]);
+      }
+      for (int it = threadIdx.x; it < rows + nv; it += blockDim.x) {
+        float* base;
+        int stride;
+        float* tb;
+        if (it < rows) {
+          base = A + (R0 + it) * lda + K;
+          stride = 1;
+          tb = Pt + R0 + it;
+        } else {
+          base = V + K * ldv + (it - rows);
+          stride = ldv;
+          tb = Vt + (it - rows);
+        }
+        float x[BK];
+        if (kb == BK) {   // full step: straight-line loads, so they all issue before the substitution
+#pragma unroll
+          for (int j = 0; j < BK; ++j) x[j] = base[j * stride];
+        } else {
+#pragma unroll
+          for (int j = 0; j < BK; ++j) x[j] = j < kb ? base[j * stride] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < BK; ++j) {
+#pragma unroll
+          for (int i = 0; i < j; ++i) x[j] = fma(-x[i], c[j][i], x[j]);
+          x[j] *= rsv[j];
+        }
+        if (kb == BK) {
+#pragma unroll
+          for (int j = 0; j < BK; ++j) {
+            base[j * stride] = x[j];
+            tb[j * ldt] = x[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < BK; ++j)
+            if (j < kb) {
+              base[j * stride] = x[j];
+              tb[j * ldt] = x[j];
+            }
+        }
+        if (WT != nullptr && it >= rows) {   // rows K..K+kb of column it - rows: W^T row segment
+          float* w = WT + (it - rows) * ldt + K;
+          if (kb == BK) {
+            reinterpret_cast<float4*>(w)[0] = make_float4(x[0], x[1], x[2], x[3]);
+            reinterpret_cast<float4*>(w)[1] = make_float4(x[4], x[5], x[6], x[7]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < BK; ++j)
+              if (j < kb) w[j] = x[j];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int i = 0; i < BK; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j)
+          if (i < kb) A[(K + i) * lda + K + j] = c[i][j];
+    }
+    if (own && R0 < n) {
+      // 3. rank-kb update: A tiles right of the panel (A22 -= P P^T), V tiles
+      //    below it in the columns already reached (V2 -= P V1)
+      const bool active = isA ? c0 >= R0 : (r0 >= R0 && c0 < R0);
+      if (active) {   // R0 < n: a full 8-column step
+        const float* bsrc = isA ? Pt : Vt;
+        float4 a4[BK], b4[BK];
+#pragma unroll
+        for (int k = 0; k < BK; ++k) {
+          a4[k] = *reinterpret_cast<const float4*>(Pt + k * ldt + r0);
+          b4[k] = *reinterpret_cast<const float4*>(bsrc + k * ldt + c0);
+        }
+#pragma unroll
+        for (int k = 0; k < BK; ++k) {
+          const float av[4] = {a4[k].x, a4[k].y, a4[k].z, a4[k].w}, bv[4] = {b4[k].x, b4[k].y, b4[k].z, b4[k].w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
+        }
+      }
+      // 4. a tile entering the next step's panel goes back to shared memory
+      const int N1 = R0 + BK;
+      const bool flush = isA ? (c0 >= R0 && c0 < N1) : (r0 >= R0 && r0 < N1);
+      if (flush) {
+        float* dst = isA ? A : V;
+        const int ld = isA ? lda : ldv;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int r = r0 + i, cc = c0 + j;
+            if (r < n && cc < n && cc <= r) dst[r * ld + cc] = acc[i][j];
+          }
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// Products of the inverse-first float node from W^T (WT[k][r] = W[r][k], W
+// lower triangular):  F^T = W R^T (R row-major in S1: B(k, c) = R[c][k]),
+// G = W Lf (S2), y = W y (Y), as one set of warp tasks of 8 rows x 64
+// columns (lane: columns c and c + 32).  K stops at the tile's last row;
+// the W^T rows are 16-byte broadcast loads, the B elements conflict-free
+// (odd ld for the transposed R, consecutive columns otherwise).  Same
+// products in the same order as the separate cta_gemm calls: identical
+// results.  Heavy and light row tiles alternate between column groups.
+template <class BVal, class Out>
+__device__ __forceinline__ void wt_tile(int n, int r0, int cb, int ncols, const float* WT, int ldt, BVal bval,
+                                        Out out) {
+  const int lane = threadIdx.x & 31;
+  const int kend = min_i(n, r0 + 8);
+  const int c_a = cb + lane, c_b = cb + lane + 32;
+  const bool va = c_a < ncols, vb = c_b < ncols;
+  float acc[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0f;
+#pragma unroll 4
+  for (int k = 0; k < kend; ++k) {
+    const float4 w0 = *reinterpret_cast<const float4*>(WT + k * ldt + r0);
+    const float4 w1 = *reinterpret_cast<const float4*>(WT + k * ldt + r0 + 4);
+    const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    const float b0 = va ? bval(k, c_a) : 0.0f, b1 = vb ? bval(k, c_b) : 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      acc[i][0] = fma(wv[i], b0, acc[i][0]);
+      acc[i][1] = fma(wv[i], b1, acc[i][1]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (r0 + i >= n) break;
+    if (va) out(r0 + i, c_a, acc[i][0]);
+    if (vb) out(r0 + i, c_b, acc[i][1]);
+  }
+}
+
+template <bool WITH_Y>
+__device__ __forceinline__ void node_products_wt(int n, const float* WT, int ldt, const float* S1, const float* S2,
+                                                 int ld, const float* Y, int ldy, int mc, float* R, float* Lf,
+                                                 float* yi, int m, int c0y, bool right, bool left) {
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int rt = (n + 7) / 8, cg = (n + 63) / 64;
+  const int gR = right ? cg : 0, gL = left ? cg : 0, gY = WITH_Y && mc > 0 ? 1 : 0;
+  const int tasks = rt * (gR + gL + gY);
+  for (int task = warp; task < tasks; task += nw) {
+    const int g = task / rt, q = task - g * rt;
+    const int r0 = 8 * ((g & 1) ? rt - 1 - q : q);
+    if (g < gR) {
+      wt_tile(n, r0, 64 * g, n, WT, ldt, [&](int k, int c) { return S1[c * ld + k]; },
+              [&](int r, int c, float v) { R[(long long)c * n + r] = v; });   // F[c][r] = (F^T)[r][c]
+    } else if (g < gR + gL) {
+      wt_tile(n, r0, 64 * (g - gR), n, WT, ldt, [&](int k, int c) { return S2[k * ld + c]; },
+              [&](int r, int c, float v) { Lf[(long long)r * n + c] = v; });
+    } else {
+      wt_tile(n, r0, 0, mc, WT, ldt, [&](int k, int c) { return Y[k * ldy + c]; },
+              [&](int r, int c, float v) { yi[(long long)r * m + c0y + c] = v; });
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Inverse-first node (n <= kNodeGemmMaxN): factor L_i against the identity
 // only, C W = I, so W = C^{-1} comes out of the blocked solve, then every
 // other vector set is one dense GEMM with W (tensor cores for double):
@@ -163,11 +413,18 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
 // ---------------------------------------------------------------------------
 constexpr int kNodeGemmMaxN = 64;
 __host__ __device__ inline int node_gemm_ldy(int m) { return m > 0 ? even_ld(min_i(m, kMC)) : 0; }
-__host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es) {
-  return 3LL * n * gemm_ld(n, es) + (long long)n * node_gemm_ldy(m);
+// S1, W, S2 (n x ld), Y (n x ldy); float: then Pt, Vt (8 x reg_chain_ldt(n) each,
+// on 16 bytes) of the register-resident chain, and with WT_PRODUCTS the
+// W^T buffer (n x reg_chain_ldt(n))
+__host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es, bool wt = false) {
+  const long long base = 3LL * n * gemm_ld(n, es) + (long long)n * node_gemm_ldy(m);
+  return es == 4 ? base + 4 + (16LL + (wt ? n : 0)) * reg_chain_ldt(n) : base;
 }
 
-template <typename T, bool WITH_Y, bool INV>
+// WT_PRODUCTS (float, with REG_CHAIN): the chain also writes W^T and the
+// three products run as node_products_wt (levels of at most one wave of CTAs:
+// the W^T buffer costs occupancy).
+template <typename T, bool WITH_Y, bool INV, bool REG_CHAIN = true, bool WT_PRODUCTS = false>
 __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level& lv, int b, int t,
                                                unsigned char* smem_raw) {
   constexpr int es = sizeof(T);
@@ -180,6 +437,10 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   T* S2 = W + n * ld;
   T* Y = S2 + n * ld;
   T* Li = p.Lb(b, i);
+  // float: operand rows of the register-resident chain, after Y on 16 bytes
+  float* Pt = reinterpret_cast<float*>(smem_raw + ((((long long)(3 * n * ld + n * ldy)) * sizeof(T) + 15) & ~15LL));
+  float* Vt = Pt + 8 * reg_chain_ldt(n);
+  float* WT = Vt + 8 * reg_chain_ldt(n);
   T* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
   T* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
   T* yi = WITH_Y ? p.Xb(b, i) : nullptr;
@@ -190,12 +451,29 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
     const int r = e / n, c = e - r * n;
     W[r * ld + c] = r == c ? T(1) : T(0);
   }
+  bool wt_ok = false;
+  if constexpr (sizeof(T) == 4 && REG_CHAIN && WT_PRODUCTS) {
+    wt_ok = reg_chain_ok(n, blockDim.x);
+    if (wt_ok)
+      for (int e = threadIdx.x; e < n * reg_chain_ldt(n); e += blockDim.x) WT[e] = 0.0f;
+  }
   cp_async_wait_all();
   __syncthreads();
-  cta_chol_solve<T, true, true>(S1, ld, n, W, ld, n);   // lower(S1) = C, W = C^{-1} (zeros above)
+  // lower(S1) = C, W = C^{-1} (zeros above)
+  if constexpr (sizeof(T) == 4 && REG_CHAIN) {
+    if (!cta_chol_inv_regs(S1, ld, n, W, ld, Pt, Vt, wt_ok ? WT : nullptr))
+      cta_chol_solve<T, true, true>(S1, ld, n, W, ld, n);
+  } else {
+    cta_chol_solve<T, true, true>(S1, ld, n, W, ld, n);
+  }
   check_factor(p, b, i, S1, ld);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
+    if constexpr (sizeof(T) == 4 && WT_PRODUCTS)
+      if (wt_ok) {
+        Li[e] = c <= r ? S1[r * ld + c] : (INV ? WT[r * reg_chain_ldt(n) + c] : 0.0f);
+        continue;
+      }
     Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : T(0));
   }
   __syncthreads();
@@ -204,6 +482,12 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   if (WITH_Y) async_load(Y, ldy, yi, n, mc0, p.m);
   cp_async_wait_all();
   __syncthreads();
+  if constexpr (sizeof(T) == 4 && WT_PRODUCTS) {
+    if (wt_ok && (!WITH_Y || p.m <= kMC)) {
+      node_products_wt<WITH_Y>(n, WT, reg_chain_ldt(n), S1, S2, ld, Y, ldy, mc0, R, Lf, yi, p.m, 0, right, left);
+      return;
+    }
+  }
   // F[r][c] = sum_k R[r][k] W[c][k]
   if (right)
     cta_gemm<T, false, true>(n, n, n, S1, ld, W, ld, [&](int r, int c, T v) { R[(long long)r * n + c] = v; });
@@ -238,7 +522,7 @@ __host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int 
   return node_uses_gemm(n) ? smem_node_gemm_elems(n, m_y, es) : smem_node_elems(n, es);
 }
 
-template <typename T, bool WITH_Y, bool INV = false>
+template <typename T, bool WITH_Y, bool INV = false, bool WT_PRODUCTS = false>
 __global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
@@ -247,7 +531,7 @@ __global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
   if (!p.active(b)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (node_uses_gemm(p.n))
-    node_gemm_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw);
+    node_gemm_body<T, WITH_Y, INV, true, WT_PRODUCTS>(p, lv, b, t, smem_raw);
   else
     node_body<T, WITH_Y, INV>(p, lv, b, t, smem_raw, node_chunk(p.n, sizeof(T)));
 }

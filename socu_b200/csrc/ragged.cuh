@@ -310,7 +310,7 @@ __device__ void rg_run(const RgArgs<T>& a, int ii, int ph, int chunk, unsigned c
     switch (P.kind) {
       case kRgNode: {
         const Problem<T> p = rg_problem(a, I, I.m);
-        node_gemm_body<T, true, true>(p, lv, 0, u, smem);
+        node_gemm_body<T, true, true, false>(p, lv, 0, u, smem);
         break;
       }
       case kRgUpd: {

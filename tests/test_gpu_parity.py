@@ -232,3 +232,25 @@ def test_streamed_sweeps_large_blocks(dtype, n, m):
     L, E, x = t(L_np, dtype), t(E_np, dtype), t(b_np, dtype)
     create_cholesky_factor_and_solve_launch(L, E, x, dtype=dtype, use_cuda_graph=True)()
     assert np.abs(x.double().cpu().numpy() - xo[0]).max() <= tol * scale
+
+
+@pytest.mark.parametrize("n", [48, 64, 61])
+def test_register_chain_matches_shared_chain_bitwise(n):
+    """The float inverse-first node keeps its trailing tiles in registers when
+    they fit (2 per thread: 256-thread CTAs here); with 64-thread CTAs they do
+    not and the shared-memory chain runs.  Same operations in the same order:
+    the factors and solutions must agree bit for bit, and with the oracle."""
+    from socu_b200.block_tridiag_solver import _launch_with_settings
+
+    N, m = 29, 5
+    L0, E0, b0 = generators.readme_problem(N, n, m, shift=10.0 + 2.0 * np.sqrt(n), seed=7 + n)
+    outs = []
+    for threads in (256, 64):
+        L, E, x = (torch.tensor(a, dtype=torch.float32, device=DEV) for a in (L0, E0, b0))
+        _launch_with_settings("factor_and_solve", L, E, x, torch.float32, {"node_threads": threads})()
+        torch.cuda.synchronize()
+        outs.append((L, E, x))
+    for a, b in zip(outs[0], outs[1]):
+        assert torch.equal(a, b)
+    x_ref = nd.nd_factor_and_solve(L0, E0, b0)[2][0]
+    assert np.abs(outs[0][2].double().cpu().numpy() - x_ref).max() <= 1e-4 * max(1.0, np.abs(x_ref).max())
