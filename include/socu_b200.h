@@ -380,9 +380,10 @@ int socu_ragged_destroy(socu_ragged_t batch);
  * counterpart in the reference. */
 int socu_dmma_peak_launch(int64_t blocks, int threads, int iters, double* sink, void* stream, double* flops);
 
-/* Error word of the tensor-core (tcgen05) kernels on the current device
- * (synchronises): 0 ok, 1 a tensor-core wait ran out (that kernel skipped its
- * result).  reset != 0 clears it afterwards.  No counterpart in the reference. */
+/* Error word of the asynchronous units on the current device (synchronises):
+ * 0 ok, 1 a tensor-core (tcgen05) wait ran out, 2 a TMA copy wait of the
+ * resident sweeps ran out (that kernel skipped its result).  reset != 0 clears
+ * it afterwards.  No counterpart in the reference. */
 int socu_tc_error(int* flag, int reset);
 
 /* Self-test of the tensor-core (tcgen05) building block of the float path:
