@@ -47,7 +47,7 @@ RAGGED_COUNT, RAGGED_SEED = 4096, 0
 # DRAM bytes (read + write) per k_bwd<float, resident, inverse> launch, averaged
 # over one backward sweep of this workload, from the ncu capture summarised in
 # profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md
-TRAFFIC_BYTES = 5005218
+TRAFFIC_BYTES = 5057908
 TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd_f32_inverse_sweep_N1024_n64_m8.md"
 # DRAM bytes (read + write) per k_node<float, y, inverse> launch of a float
 # factor_and_solve of this shape, averaged over its 11 levels: ncu capture of

@@ -418,7 +418,9 @@ __host__ __device__ inline int node_gemm_ldy(int m) { return m > 0 ? even_ld(min
 // W^T buffer (n x reg_chain_ldt(n))
 __host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es, bool wt = false) {
   const long long base = 3LL * n * gemm_ld(n, es) + (long long)n * node_gemm_ldy(m);
-  return es == 4 ? base + 4 + (16LL + (wt ? n : 0)) * reg_chain_ldt(n) : base;
+  // WT_PRODUCTS also keeps a buffer for R, loaded during the chain
+  return es == 4 ? base + 4 + (16LL + (wt ? n : 0)) * reg_chain_ldt(n) + (wt ? (long long)n * gemm_ld(n, es) : 0)
+                 : base;
 }
 
 // WT_PRODUCTS (float, with REG_CHAIN): the chain also writes W^T and the
@@ -441,23 +443,35 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
   float* Pt = reinterpret_cast<float*>(smem_raw + ((((long long)(3 * n * ld + n * ldy)) * sizeof(T) + 15) & ~15LL));
   float* Vt = Pt + 8 * reg_chain_ldt(n);
   float* WT = Vt + 8 * reg_chain_ldt(n);
+  float* Rb = WT + n * reg_chain_ldt(n);   // WT_PRODUCTS: R, loaded during the chain
   T* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
   T* Lf = left ? p.Eb(b, lv.oc + 2 * t - 1) : nullptr;
   T* yi = WITH_Y ? p.Xb(b, i) : nullptr;
+  bool wt_ok = false;
+  if constexpr (sizeof(T) == 4 && REG_CHAIN && WT_PRODUCTS) wt_ok = reg_chain_ok(n, blockDim.x) && (!WITH_Y || p.m <= kMC);
 
   async_load(S1, ld, Li, n, n, n);
+  if (wt_ok) cp_async_commit();                // the chain waits for L_i only
   if (left) async_load(S2, ld, Lf, n, n, n);   // prefetch: S2 is untouched by the factor
+  if constexpr (sizeof(T) == 4 && WT_PRODUCTS) {
+    if (wt_ok) {
+      if (right) async_load(Rb, ld, R, n, n, n);
+      if (WITH_Y) async_load(Y, ldy, yi, n, p.m, p.m);
+      cp_async_commit();
+    }
+  }
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
     W[r * ld + c] = r == c ? T(1) : T(0);
   }
-  bool wt_ok = false;
   if constexpr (sizeof(T) == 4 && REG_CHAIN && WT_PRODUCTS) {
-    wt_ok = reg_chain_ok(n, blockDim.x);
     if (wt_ok)
       for (int e = threadIdx.x; e < n * reg_chain_ldt(n); e += blockDim.x) WT[e] = 0.0f;
   }
-  cp_async_wait_all();
+  if (wt_ok)
+    cp_async_wait_one();
+  else
+    cp_async_wait_all();
   __syncthreads();
   // lower(S1) = C, W = C^{-1} (zeros above)
   if constexpr (sizeof(T) == 4 && REG_CHAIN) {
@@ -476,18 +490,20 @@ __device__ __forceinline__ void node_gemm_body(const Problem<T>& p, const Level&
       }
     Li[e] = c <= r ? S1[r * ld + c] : (INV ? W[c * ld + r] : T(0));
   }
-  __syncthreads();
   const int mc0 = WITH_Y ? min_i(kMC, p.m) : 0;
+  if constexpr (sizeof(T) == 4 && WT_PRODUCTS) {
+    if (wt_ok) {   // R, Lf and y arrived during the chain
+      cp_async_wait_all();
+      __syncthreads();
+      node_products_wt<WITH_Y>(n, WT, reg_chain_ldt(n), Rb, S2, ld, Y, ldy, mc0, R, Lf, yi, p.m, 0, right, left);
+      return;
+    }
+  }
+  __syncthreads();
   if (right) async_load(S1, ld, R, n, n, n);
   if (WITH_Y) async_load(Y, ldy, yi, n, mc0, p.m);
   cp_async_wait_all();
   __syncthreads();
-  if constexpr (sizeof(T) == 4 && WT_PRODUCTS) {
-    if (wt_ok && (!WITH_Y || p.m <= kMC)) {
-      node_products_wt<WITH_Y>(n, WT, reg_chain_ldt(n), S1, S2, ld, Y, ldy, mc0, R, Lf, yi, p.m, 0, right, left);
-      return;
-    }
-  }
   // F[r][c] = sum_k R[r][k] W[c][k]
   if (right)
     cta_gemm<T, false, true>(n, n, n, S1, ld, W, ld, [&](int r, int c, T v) { R[(long long)r * n + c] = v; });
