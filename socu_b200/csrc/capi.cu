@@ -155,13 +155,13 @@ int sm_count() {
   return sms;
 }
 
-template <typename K>
-int level_threads(K kernel, int nth, long long blocks, size_t smem) {
+template <typename K, class Smem>
+int level_threads(K kernel, int nth, long long blocks, Smem smem) {
   if (nth != 256 || blocks <= 0) return nth;
   int dev = 0;
   const int sms = sm_count();
   if (sms <= 0 || cudaGetDevice(&dev) != cudaSuccess) return nth;
-  const int o256 = occupancy(kernel, dev, 256, smem), o128 = occupancy(kernel, dev, 128, smem);
+  const int o256 = occupancy(kernel, dev, 256, smem(256)), o128 = occupancy(kernel, dev, 128, smem(128));
   if (o256 <= 0 || o128 <= 0) return nth;
   const long long w256 = (blocks + (long long)sms * o256 - 1) / ((long long)sms * o256);
   const long long w128 = (blocks + (long long)sms * o128 - 1) / ((long long)sms * o128);
@@ -494,7 +494,11 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   const int K = lv.K;
   for (int l = 0; l < K; ++l) lv.lv[l].tile = tile;
   const bool withY = op == SOCU_OP_FACTOR_AND_SOLVE;
-  const size_t sd = smem_node_launch_elems(n, withY ? p.m : 0, sizeof(T)) * sizeof(T);
+  // node shared memory by CTA size (the register-resident chain's buffers only where it runs)
+  auto node_smem = [&](int threads) {
+    return (size_t)smem_node_launch_elems(n, withY ? p.m : 0, sizeof(T), threads) * sizeof(T);
+  };
+  const size_t sd = node_smem(256);   // the largest
   const size_t su = smem_update_launch_elems(n, sizeof(T), tile) * sizeof(T);
   const int mm = p.m > 0 ? p.m : 1;
   const bool res = (long long)smem_sweep_res_elems(n, mm) * (long long)sizeof(T) <= (long long)max_smem_optin();
@@ -583,7 +587,7 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   if (run && res) maps = sweep_maps(p);
   auto node_threads = [&](long long blocks) {
     if (cfg.node_threads) return cfg.node_threads;
-    return run ? level_threads(node_kernel, nth, blocks, sd) : nth;
+    return run ? level_threads(node_kernel, nth, blocks, node_smem) : nth;
   };
   const bool forked = run && fork != nullptr && fork->ok();
 
@@ -623,9 +627,12 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
         else if (node_wt)
           go_on(st, node_wt_kernel, SOCU_KIND_NODE, node_blocks, sd_wt, L, nthr);
         else
-          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, nthr);
+          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, node_smem(nthr), L, nthr);
       } else {
-        go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, sd, L, node_threads(node_blocks));
+        {
+          const int nthr = node_threads(node_blocks);
+          go_on(st, node_kernel, SOCU_KIND_NODE, node_blocks, node_smem(nthr), L, nthr);
+        }
       }
       if (l + 1 < K) {
         // fused forward: apply this level's updates to every target vector
@@ -1209,7 +1216,7 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
   // shared memory: the largest body at the largest block size (n <= 64: the
   // inverse-first node body)
   r->vc = maxnv;
-  size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es) * es;
+  size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es, false, false) * es;   // ragged nodes: shared-memory chain
   smem = std::max(smem, (size_t)smem_update_full_elems(maxn, es) * es);
   smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
   if (r->refine) smem = std::max(smem, (size_t)smem_residual_rows_elems(maxn) * sizeof(double));

@@ -453,6 +453,70 @@ __device__ __forceinline__ void rank_update_simt(T* A, int lda, T* V, int ldv, i
   }
 }
 
+// Float rank-kb update with the solved panel also held transposed in Pt
+// (Pt[k * ldt + row], written by the item solves): the row operand of every
+// tile and the column operand of the A22 tiles are 16-byte loads of
+// consecutive rows, and with VEC_V (ldv a multiple of 4) the vector operand
+// too.  Same tiles, values and order as rank_update_simt: identical results.
+template <bool VEC_V>
+__device__ __forceinline__ void rank_update_simt_pt(float* A, int lda, float* V, int ldv, int n, int K, int kb,
+                                                    int R0, int nv, bool factor, const float* Pt, int ldt) {
+  constexpr int BK = 8;
+  const int M = n - R0;
+  const int tm = (M + 3) / 4;
+  const int tnA = factor ? (M + 3) / 4 : 0, tnV = (nv + 3) / 4;
+  const int nA = tm * tnA, total = nA + tm * tnV;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const bool isA = idx < nA;
+    const int tt = isA ? idx : idx - nA;
+    const int tn = isA ? tnA : tnV;
+    const int r0 = (tt / tn) * 4, c0 = (tt % tn) * 4;
+    if (isA && c0 > r0 + 3) continue;
+    float* C = isA ? A + R0 * lda + R0 : V + R0 * ldv;
+    const int ldc = isA ? lda : ldv;
+    const int N = isA ? M : nv;
+    float acc[4][4];
+    int ra[4], cb[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) ra[i] = min(r0 + i, M - 1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cb[j] = min(c0 + j, N - 1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = C[ra[i] * ldc + cb[j]];
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      if (k < kb) {
+        const float4 a4 = *reinterpret_cast<const float4*>(Pt + k * ldt + R0 + r0);
+        const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+        float b[4];
+        if (isA) {
+          const float4 b4 = *reinterpret_cast<const float4*>(Pt + k * ldt + R0 + c0);
+          b[0] = b4.x; b[1] = b4.y; b[2] = b4.z; b[3] = b4.w;
+        } else if (VEC_V) {
+          const float4 b4 = *reinterpret_cast<const float4*>(V + (K + k) * ldv + c0);
+          b[0] = b4.x; b[1] = b4.y; b[2] = b4.z; b[3] = b4.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) b[j] = V[(K + k) * ldv + cb[j]];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(-a[i], b[j], acc[i][j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = r0 + i, c = c0 + j;
+        if (r < M && c < N && (!isA || c <= r)) C[r * ldc + c] = acc[i][j];
+      }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // CTA: blocked right-looking Cholesky of the n x n block in A fused with the
 // solve C V = V for nv vectors (columns of V), by 8-column blocks.
@@ -469,8 +533,10 @@ __device__ __forceinline__ void rank_update_simt(T* A, int lda, T* V, int ldv, i
 // IDENTITY: V starts as the n x n identity (nv = n), so it ends as C^{-1}.
 // Rows [K, K+kb) of column c are still zero for c >= K+kb, which leaves those
 // columns out of the item solves and of the trailing update.
+// Pt (float, optional, 8 x ldt with ldt >= n rounded up to 4 + 4, 16-byte
+// aligned): transposed copy of each solved panel for rank_update_simt_pt.
 template <typename T, bool FACTOR, bool IDENTITY = false>
-__device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
+__device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv, float* Pt = nullptr, int ldt = 0) {
   // diagonal block width: the whole block lives in every thread's registers
   // and is factored redundantly by every thread (work grows as BK^3 x threads)
   constexpr int BK = 8;
@@ -529,7 +595,21 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
 #pragma unroll
       for (int j = 0; j < BK; ++j)
         if (j < kb) base[j * stride] = x[j];
+      if constexpr (sizeof(T) == 4)
+        if (Pt != nullptr && it < rows) {
+#pragma unroll
+          for (int j = 0; j < BK; ++j)
+            if (j < kb) Pt[j * ldt + R0 + it] = x[j];
+        }
     }
+    }
+    if constexpr (sizeof(T) == 4 && !FACTOR) {
+      // solve-only pass: the panel is the stored factor's; copy it transposed
+      if (Pt != nullptr)
+        for (int e = threadIdx.x; e < (n - R0) * kb; e += blockDim.x) {
+          const int r = e / kb, j = e - r * kb;
+          Pt[j * ldt + R0 + r] = A[(R0 + r) * lda + K + j];
+        }
     }
     __syncthreads();
     // 3. write the factored diagonal block (one thread, static register
@@ -542,10 +622,18 @@ __device__ void cta_chol_solve(T* A, int lda, int n, T* V, int ldv, int nv) {
           if (i < kb) A[(K + i) * lda + K + j] = c[i][j];
     }
     if (R0 < n) {
-      if constexpr (sizeof(T) == 8)
+      if constexpr (sizeof(T) == 8) {
         rank_update_f64(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR);
-      else
-        rank_update_simt<T>(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR);
+      } else {
+        if (Pt != nullptr) {
+          if ((ldv & 3) == 0 && (reinterpret_cast<uintptr_t>(V) & 15) == 0)
+            rank_update_simt_pt<true>(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR, Pt, ldt);
+          else
+            rank_update_simt_pt<false>(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR, Pt, ldt);
+        } else {
+          rank_update_simt<T>(A, lda, V, ldv, n, K, kb, R0, nv, FACTOR);
+        }
+      }
     }
     __syncthreads();
   }

@@ -41,8 +41,17 @@ __host__ __device__ inline int gemm_ld(int n, int es) { return es == 8 ? ((n + 1
 // (n > 64: 64 for float -- two CTAs per SM, measured faster than one pass of
 // all vectors at one CTA per SM -- and 80 for double, the most that fit)
 __host__ __device__ inline int node_chunk(int n, int es) { return n <= 64 ? 232 : (es == 4 ? 64 : 80); }
+// float: vector rows on 16 bytes (4-wide operand loads in the rank updates),
+// then the transposed panel Pt (8 x node_ldt(n)) of cta_chol_solve
+__host__ __device__ inline int node_vld(int vc, int es) { return es == 8 ? gemm_ld(vc, es) : ((vc + 3) & ~3) + 4; }
+__host__ __device__ inline int node_ldt(int n) { return ((n + 3) & ~3) + 4; }
+__host__ __device__ inline long long node_v_off(int n, int es) {
+  const long long a = (long long)n * gemm_ld(n, es);
+  return es == 4 ? ((a + 3) & ~3LL) : a;
+}
 __host__ __device__ inline long long smem_node_elems(int n, int es) {
-  return (long long)n * gemm_ld(n, es) + (long long)n * gemm_ld(node_chunk(n, es), es);
+  const long long v = node_v_off(n, es) + (long long)n * node_vld(node_chunk(n, es), es);
+  return es == 4 ? v + 8LL * node_ldt(n) : v;
 }
 __host__ __device__ inline int update_ld(int k, int es) { return gemm_ld(k, es); }
 // blocked Schur update (n > 64) with tile x tile output tiles
@@ -88,9 +97,10 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
   const bool right = i + s < p.N, left = t >= 1;
   const int nr = right ? n : 0, nl = left ? n : 0, ny = WITH_Y ? p.m : 0, ni = INV ? n : 0;
   const int NV = nr + nl + ny + ni;
-  const int lda = gemm_ld(n, es), ldv = gemm_ld(vc, es);
+  const int lda = gemm_ld(n, es), ldv = node_vld(vc, es);
   T* A = reinterpret_cast<T*>(smem_raw);
-  T* V = A + n * lda;
+  T* V = A + node_v_off(n, es);
+  float* Pt = es == 4 ? reinterpret_cast<float*>(V + (long long)n * ldv) : nullptr;
 
   T* Li = p.Lb(b, i);
   T* R = right ? p.Eb(b, lv.oc + 2 * t) : nullptr;
@@ -130,7 +140,7 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
   if (NV > 0) chunk_io(0, true);
   cp_async_wait_all();
   __syncthreads();
-  cta_chol_solve<T, true>(A, lda, n, V, ldv, min_i(NV, vc));
+  cta_chol_solve<T, true>(A, lda, n, V, ldv, min_i(NV, vc), Pt, node_ldt(n));
   check_factor(p, b, i, A, lda);
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - r * n;
@@ -143,7 +153,7 @@ __device__ __forceinline__ void node_body(const Problem<T>& p, const Level& lv, 
     chunk_io(v0, true);
     cp_async_wait_all();
     __syncthreads();
-    cta_chol_solve<T, false>(A, lda, n, V, ldv, min_i(NV - v0, vc));
+    cta_chol_solve<T, false>(A, lda, n, V, ldv, min_i(NV - v0, vc), Pt, node_ldt(n));
     chunk_io(v0, false);
   }
 }
@@ -416,11 +426,13 @@ __host__ __device__ inline int node_gemm_ldy(int m) { return m > 0 ? even_ld(min
 // S1, W, S2 (n x ld), Y (n x ldy); float: then Pt, Vt (8 x reg_chain_ldt(n) each,
 // on 16 bytes) of the register-resident chain, and with WT_PRODUCTS the
 // W^T buffer (n x reg_chain_ldt(n))
-__host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es, bool wt = false) {
+// reg: the launch's CTAs are large enough for the register-resident chain
+// (reg_chain_ok), which needs Pt / Vt; wt implies reg.
+__host__ __device__ inline long long smem_node_gemm_elems(int n, int m, int es, bool wt = false, bool reg = true) {
   const long long base = 3LL * n * gemm_ld(n, es) + (long long)n * node_gemm_ldy(m);
+  if (es != 4 || !(reg || wt)) return base;
   // WT_PRODUCTS also keeps a buffer for R, loaded during the chain
-  return es == 4 ? base + 4 + (16LL + (wt ? n : 0)) * reg_chain_ldt(n) + (wt ? (long long)n * gemm_ld(n, es) : 0)
-                 : base;
+  return base + 4 + (16LL + (wt ? n : 0)) * reg_chain_ldt(n) + (wt ? (long long)n * gemm_ld(n, es) : 0);
 }
 
 // WT_PRODUCTS (float, with REG_CHAIN): the chain also writes W^T and the
@@ -534,8 +546,9 @@ __global__ void k_info_reset(int* info, int B) {
 __host__ __device__ inline bool node_uses_gemm(int n) { return n <= kNodeGemmMaxN; }
 __host__ __device__ inline bool inv_first_node(int n) { return node_uses_gemm(n); }
 // dynamic shared memory (elements) of k_node; m_y = right-hand sides solved in the node (0 without y)
-__host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int es) {
-  return node_uses_gemm(n) ? smem_node_gemm_elems(n, m_y, es) : smem_node_elems(n, es);
+__host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int es, int threads = 256) {
+  return node_uses_gemm(n) ? smem_node_gemm_elems(n, m_y, es, false, reg_chain_ok(n, threads))
+                           : smem_node_elems(n, es);
 }
 
 template <typename T, bool WITH_Y, bool INV = false, bool WT_PRODUCTS = false>
