@@ -1120,7 +1120,6 @@ namespace {
 // ragged batches
 // ---------------------------------------------------------------------------
 constexpr int kRgMaxBlock = 64;                 // resident sweeps with diagonal inverses
-constexpr int kRgThreads = 128;   // 3 CTAs per SM at n = 48 (shared-memory bound) instead of 2
 constexpr long long kRgTimeoutNs = 4000000000LL;   // bound of one queue wait (4 s)
 
 int rg_upc(int n) { return n <= 8 ? 8 : (n <= 16 ? 4 : (n <= 32 ? 2 : 1)); }
@@ -1216,7 +1215,7 @@ int rg_create(socu_ragged_s* r, const int64_t* horizon, const int64_t* n, const 
   // shared memory: the largest body at the largest block size (n <= 64: the
   // inverse-first node body)
   r->vc = maxnv;
-  size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es, false, false) * es;   // ragged nodes: shared-memory chain
+  size_t smem = (size_t)smem_node_gemm_elems(maxn, maxm, es, false, false) * es;   // ragged nodes: shared-memory chain (measured faster there)
   smem = std::max(smem, (size_t)smem_update_full_elems(maxn, es) * es);
   smem = std::max(smem, (size_t)smem_sweep_res_elems(maxn, maxm) * es);
   if (r->refine) smem = std::max(smem, (size_t)smem_residual_rows_elems(maxn) * sizeof(double));
