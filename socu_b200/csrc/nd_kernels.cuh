@@ -552,7 +552,7 @@ __host__ __device__ inline long long smem_node_launch_elems(int n, int m_y, int 
 }
 
 template <typename T, bool WITH_Y, bool INV = false, bool WT_PRODUCTS = false>
-__global__ void __launch_bounds__(256, 2) k_node(Problem<T> p, Level lv) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_node(Problem<T> p, Level lv) {
   const int b = blockIdx.x / lv.d;
   const int t = blockIdx.x - b * lv.d;
   pdl_wait();
