@@ -653,8 +653,16 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
           }
         }
         if (!tc_done) {
+          // whole-block updates on levels with at most one block per SM: one
+          // 32 x 32 tile per CTA instead (identical results), spread over the SMs
+          const size_t su_tile = (size_t)smem_update_tile_elems(n, sizeof(T)) * sizeof(T);
+          const bool upd_tiles = run && update_uses_full(n) && cfg.update_threads == 0 && sms > 0 &&
+                                 upd_blocks <= sms && prepare(k_update_tiles<T>, su_tile) == cudaSuccess;
           if (update_uses_big(n))
             go_on(st, k_update_big<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, 256);
+          else if (upd_tiles)
+            go_on(st, k_update_tiles<T>, SOCU_KIND_UPDATE, (long long)p.B * update_tile_tasks(n, p.N, L), su_tile,
+                  L, kUpdTileThreads);
           else
             go_on(st, k_update<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, upd_thr);
         }
