@@ -415,6 +415,7 @@ Problem<T> make_problem(void* L, void* E, void* x, const uint8_t* mask, const Di
   p.X = static_cast<T*>(x);
   p.mask = mask;
   p.info = nullptr;
+  p.xacc = nullptr;
   p.B = d.B;
   p.N = d.N;
   p.n = d.n;
@@ -847,16 +848,12 @@ RefineArgs refine_args(const double* L, const double* E, const double* b, double
 
 // One refinement round after a solve that left delta in R32: x += delta,
 // FP64 residual (R32 = r, norms), convergence test.
+// (x += delta happened in the float solve's backward sweep: Problem::xacc)
 int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) {
   if (count == nullptr) {
-    const long long nvec = (long long)a.B * a.N * a.n * a.m;
-    const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
     const int nrc = ceil_div(a.n, kResRows);
     // each kernel follows the previous one of the round on the same stream
     const bool pdl = g_prof == nullptr;
-    prof_begin(st, SOCU_KIND_REFINE_UPDATE);
-    launch(k_ref_update, (unsigned)upd_blocks, 256, 0, st, pdl, a);
-    prof_end(st);
     prof_begin(st, SOCU_KIND_RESIDUAL);
     if (residual_uses_rows(a.n)) {
       const cudaError_t e = launch_residual_rows<true>(a, st, pdl);
@@ -869,7 +866,7 @@ int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) 
     launch(k_ref_check, (unsigned)((a.B + 255) / 256), 256, 0, st, pdl, a);
     prof_end(st);
   } else {
-    *count = 3;
+    *count = 2;
   }
   return SOCU_OK;
 }
@@ -881,6 +878,7 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
+  pf.xacc = a.x;   // the backward sweep adds delta to x (x = 0 after the reset)
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
@@ -922,6 +920,7 @@ int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
+  pf.xacc = a.x;   // the backward sweep adds delta to x
   long long c = 0, cr = 0;
   int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (s != SOCU_OK) return s;

@@ -1611,6 +1611,19 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv, const __gri
 // ---------------------------------------------------------------------------
 // k_bwd (level l, descending): x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
 // ---------------------------------------------------------------------------
+// store_block, and with xacc also xacc[r * dst_ld + c] += dst value (in FP64)
+template <typename T>
+__device__ __forceinline__ void store_block_acc(T* dst, long long dst_ld, const T* src, int ld, int rows, int cols,
+                                                double* xacc) {
+  const int total = rows * cols;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int r = e / cols, c = e - r * cols;
+    const T v = src[r * ld + c];
+    dst[(long long)r * dst_ld + c] = v;
+    if (xacc != nullptr) xacc[(long long)r * dst_ld + c] += (double)v;
+  }
+}
+
 template <typename T, bool RES, bool INV>
 __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, int b, int t,
                                          unsigned char* smem_raw, const SweepMaps* tm = nullptr) {
@@ -1636,6 +1649,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
   const T* G = left ? p.Eb(b, slot - 1) : nullptr;
   const T* Li = p.Lb(b, i);
   T* xi = p.Xb(b, i);
+  double* xa = p.xacc == nullptr ? nullptr : p.xacc + (long long)b * p.sX + (long long)i * n * p.m;
   const ResTma tu = RES ? res_tma_begin(tm, smem_raw, bar) : ResTma{false, false};
   if (!lv.pre) pdl_wait();
   if (RES) {
@@ -1693,7 +1707,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
         else
           res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
         __syncthreads();
-        store_block(xi + c0, p.m, Z1, ldy, n, mc);
+        store_block_acc(xi + c0, p.m, Z1, ldy, n, mc, xa == nullptr ? nullptr : xa + c0);
         continue;
       }
       res_tri_solve<T, true>(Y, ldy, mc, Cs, ldm, dv, n);
@@ -1701,7 +1715,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
       sweep_accumulate2<T, true, false>(Y, Z1, F, Z2, G, ldy, mc, n, Ms);
       sweep_upper_solve(Y, ldy, mc, Li, n, Ms, dv);
     }
-    store_block(xi + c0, p.m, Y, ldy, n, mc);
+    store_block_acc(xi + c0, p.m, Y, ldy, n, mc, xa == nullptr ? nullptr : xa + c0);
   }
 }
 

@@ -250,6 +250,7 @@ __device__ __forceinline__ Problem<T> rg_problem(const RgArgs<T>& a, const RgIns
   p.X = a.X + I.oX;
   p.mask = nullptr;
   p.info = nullptr;
+  p.xacc = nullptr;
   p.B = 1;
   p.N = I.N;
   p.n = I.n;

@@ -137,18 +137,6 @@ __global__ void __launch_bounds__(256) k_ref_init(RefineArgs a) {
   ref_init_body(a, bi, i);
 }
 
-// x += delta (R32) for active instances; grid-stride over the whole batch.
-__global__ void __launch_bounds__(256) k_ref_update(RefineArgs a) {
-  pdl_wait();
-  pdl_trigger();
-  const long long per = (long long)a.N * a.n * a.m;
-  const long long total = (long long)a.B * per;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int bi = (int)(e / per);
-    if (a.active[bi]) a.x[e] += (double)a.R32[e];
-  }
-}
 
 // r = b - Psi x for rows [r0, r0+32) of block row i (FP64 against the
 // original blocks), R32 = float(r), ||r||_inf and ||x||_inf accumulated.
