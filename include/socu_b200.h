@@ -196,10 +196,10 @@ typedef enum socu_kernel_kind {
   SOCU_KIND_FORWARD = 3,       /* forward sweep */
   SOCU_KIND_BACKWARD = 4,      /* backward sweep */
   SOCU_KIND_REFINE_SETUP = 5,  /* refinement: state reset, float copies, norms */
-  SOCU_KIND_REFINE_UPDATE = 6, /* refinement: x += delta (not a separate kernel any more: the float
-                                  solve's backward sweep adds each final delta block to x) */
+  SOCU_KIND_REFINE_UPDATE = 6, /* refinement: x += delta */
   SOCU_KIND_RESIDUAL = 7,      /* refinement: FP64 residual and norms */
-  SOCU_KIND_REFINE_CHECK = 8,  /* refinement: convergence test */
+  SOCU_KIND_REFINE_CHECK = 8,  /* refinement: convergence test (not a separate kernel any more: the
+                                  residual kernel's last CTA per instance runs it) */
   SOCU_KIND_RAGGED = 9,        /* ragged batch: queue reset + persistent solver */
   SOCU_KIND_COUNT = 10
 } socu_kernel_kind;

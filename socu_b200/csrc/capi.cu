@@ -415,7 +415,6 @@ Problem<T> make_problem(void* L, void* E, void* x, const uint8_t* mask, const Di
   p.X = static_cast<T*>(x);
   p.mask = mask;
   p.info = nullptr;
-  p.xacc = nullptr;
   p.B = d.B;
   p.N = d.N;
   p.n = d.n;
@@ -654,16 +653,8 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
           }
         }
         if (!tc_done) {
-          // whole-block updates on levels with at most one block per SM: one
-          // 32 x 32 tile per CTA instead (identical results), spread over the SMs
-          const size_t su_tile = (size_t)smem_update_tile_elems(n, sizeof(T)) * sizeof(T);
-          const bool upd_tiles = run && update_uses_full(n) && cfg.update_threads == 0 && sms > 0 &&
-                                 upd_blocks <= sms && prepare(k_update_tiles<T>, su_tile) == cudaSuccess;
           if (update_uses_big(n))
             go_on(st, k_update_big<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, 256);
-          else if (upd_tiles)
-            go_on(st, k_update_tiles<T>, SOCU_KIND_UPDATE, (long long)p.B * update_tile_tasks(n, p.N, L), su_tile,
-                  L, kUpdTileThreads);
           else
             go_on(st, k_update<T>, SOCU_KIND_UPDATE, upd_blocks, su, L, upd_thr);
         }
@@ -843,27 +834,33 @@ RefineArgs refine_args(const double* L, const double* E, const double* b, double
   a.eta = eta; a.iters = iters; a.rout = nullptr;
   a.B = d.B; a.N = d.N; a.n = d.n; a.m = d.m; a.S = d.S;
   a.tol = tol; a.max_iter = max_iter;
+  a.check_in_residual = 0;
   return a;
 }
 
 // One refinement round after a solve that left delta in R32: x += delta,
 // FP64 residual (R32 = r, norms), convergence test.
-// (x += delta happened in the float solve's backward sweep: Problem::xacc)
+// x += delta, then the residual, whose last CTA per instance also runs the
+// convergence test (RefineArgs::check_in_residual)
 int refine_finish_round(const RefineArgs& a, cudaStream_t st, long long* count) {
   if (count == nullptr) {
+    const long long nvec = (long long)a.B * a.N * a.n * a.m;
+    const int upd_blocks = (int)((nvec + 255) / 256 < 148 * 16 ? (nvec + 255) / 256 : 148 * 16);
     const int nrc = ceil_div(a.n, kResRows);
     // each kernel follows the previous one of the round on the same stream
     const bool pdl = g_prof == nullptr;
+    prof_begin(st, SOCU_KIND_REFINE_UPDATE);
+    launch(k_ref_update, (unsigned)upd_blocks, 256, 0, st, pdl, a);
+    prof_end(st);
+    RefineArgs ac = a;
+    ac.check_in_residual = 1;
     prof_begin(st, SOCU_KIND_RESIDUAL);
     if (residual_uses_rows(a.n)) {
-      const cudaError_t e = launch_residual_rows<true>(a, st, pdl);
+      const cudaError_t e = launch_residual_rows<true>(ac, st, pdl);
       if (e != cudaSuccess) return cuda_status(e);
     } else
       launch(k_residual<true>, (unsigned)((long long)a.B * a.N * nrc), 256, smem_residual_elems(a.n) * sizeof(double),
-             st, pdl, a);
-    prof_end(st);
-    prof_begin(st, SOCU_KIND_REFINE_CHECK);
-    launch(k_ref_check, (unsigned)((a.B + 255) / 256), 256, 0, st, pdl, a);
+             st, pdl, ac);
     prof_end(st);
   } else {
     *count = 2;
@@ -878,7 +875,6 @@ int refine_prologue(const RefineArgs& a, cudaStream_t st, long long* count, cons
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
-  pf.xacc = a.x;   // the backward sweep adds delta to x (x = 0 after the reset)
   const int chk_blocks = (a.B + 255) / 256;
   if (run) {
     const size_t sres = smem_residual_elems(a.n) * sizeof(double);
@@ -920,7 +916,6 @@ int refine_iteration(const RefineArgs& a, cudaStream_t st, long long* count) {
   const bool run = count == nullptr;
   Dims d{a.B, a.N, a.n, a.m, a.S};
   Problem<float> pf = make_problem<float>(a.L32, a.E32, a.R32, a.active, d);
-  pf.xacc = a.x;   // the backward sweep adds delta to x
   long long c = 0, cr = 0;
   int s = enqueue<float>(SOCU_OP_SOLVE, pf, st, run ? nullptr : &c, use_inverse<float>(a.n, a.m));
   if (s != SOCU_OK) return s;

@@ -38,8 +38,6 @@ struct Problem {
   int* info;             // may be null: per batch entry, 0 or 1 + the first node whose pivot failed
   int B, N, n, m, S;
   long long sL, sE, sX;  // per-batch strides in elements
-  double* xacc;          // may be null: the backward sweep also adds each final x_i to xacc (same
-                         // layout as X) -- the x += delta of a refinement round
 
   __device__ __forceinline__ T* Lb(int b, int i) const {
     return L + (long long)b * sL + (long long)i * n * n;

@@ -886,87 +886,6 @@ __global__ void __launch_bounds__(256) k_update(Problem<T> p, Level lv) {
     update_body<T>(p, lv, b, task, smem_raw);
 }
 
-// n <= 64 on levels with few blocks: one 32 x 32 output tile of a target
-// (lower tiles) or fill-in block per CTA of 64 threads, so a block's update
-// spreads over several SMs instead of queueing on one SM's FP64 tensor pipe.
-// Same DMMA products, k order and rounding as update_full_body: identical
-// results.
-constexpr int kUpdTile = 32;
-constexpr int kUpdTileThreads = 64;
-__host__ __device__ inline int update_tile_tasks(int n, int N, const Level& lv) {
-  const int nt = ceil_div(n, kUpdTile);
-  return (N / (2 * lv.s)) * (nt * (nt + 1) / 2) + (lv.d - 1) * nt * nt;
-}
-__host__ __device__ inline long long smem_update_tile_elems(int n, int es) {
-  return 2LL * kUpdTile * update_full_ld(2 * n, es);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kUpdTileThreads) k_update_tiles(Problem<T> p, Level lv) {
-  constexpr int es = sizeof(T);
-  const int per_b = update_tile_tasks(p.n, p.N, lv);
-  const int b = blockIdx.x / per_b;
-  const int task = blockIdx.x - b * per_b;
-  pdl_wait();
-  pdl_trigger();
-  if (!p.active(b)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n = p.n, N = p.N, s = lv.s;
-  const int nt = ceil_div(n, kUpdTile), nlt = nt * (nt + 1) / 2;
-  const int U = N / (2 * s);
-  const int lda = update_full_ld(2 * n, es);
-  T* Ab = reinterpret_cast<T*>(smem_raw);
-  T* Bb = Ab + kUpdTile * lda;
-  auto sub = [](T* o, double v) { *o = (T)((double)*o - v); };
-  if (task < U * nlt) {
-    const int u = task / nlt + 1;
-    int ta, tc;
-    lower_tile_index(task - (u - 1) * nlt, ta, tc);
-    const int j = 2 * s * u - 1;
-    const T* F = p.Eb(b, lv.oc + 2 * (u - 1));
-    const bool hasG = j + s < N;
-    const T* G = hasG ? p.Eb(b, lv.oc + 2 * u - 1) : nullptr;
-    const int K = hasG ? 2 * n : n;
-    const int r0 = ta * kUpdTile, wa = min_i(kUpdTile, n - r0);
-    const int c0 = tc * kUpdTile, wc = min_i(kUpdTile, n - c0);
-    const bool diag = ta == tc;
-    // rows r0.. and c0.. of [F | G^T]
-    async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);
-    if (hasG) async_load_t(Ab + n, lda, G + r0, n, wa, n);
-    if (!diag) {
-      async_load(Bb, lda, F + (long long)c0 * n, wc, n, n);
-      if (hasG) async_load_t(Bb + n, lda, G + c0, n, wc, n);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    T* Lj = p.Lb(b, j);
-    auto out = [&](int r, int c, double v) { sub(Lj + (long long)(r0 + r) * n + c0 + c, v); };
-    if (diag)
-      warp_gemm_dmma<T, false, true, true>(wa, wc, K, Ab, lda, Ab, lda, out);
-    else
-      warp_gemm_dmma<T, false, true, false>(wa, wc, K, Ab, lda, Bb, lda, out);
-  } else {
-    const int f = task - U * nlt;
-    const int t = f / (nt * nt) + 1;
-    const int tt = f - (t - 1) * nt * nt;
-    const int ta = tt / nt, tc = tt - ta * nt;
-    const int i = s - 1 + 2 * s * t;
-    if (i + s >= N) return;
-    const T* F = p.Eb(b, lv.oc + 2 * t);
-    const T* G = p.Eb(b, lv.oc + 2 * t - 1);
-    T* X = p.Eb(b, lv.on + t - 1);
-    const int r0 = ta * kUpdTile, wa = min_i(kUpdTile, n - r0);
-    const int c0 = tc * kUpdTile, wc = min_i(kUpdTile, n - c0);
-    const int ldg = update_full_ld(kUpdTile, es);
-    async_load(Ab, lda, F + (long long)r0 * n, wa, n, n);   // F rows r0..
-    async_load(Bb, ldg, G + c0, n, wc, n);                    // G columns c0.., n x wc
-    cp_async_wait_all();
-    __syncthreads();
-    warp_gemm_dmma<T, false, false>(wa, wc, n, Ab, lda, Bb, ldg,
-                                    [&](int r, int c, double v) { sub(X + (long long)(r0 + r) * n + c0 + c, v); });
-  }
-}
-
 // 64 < n <= 128: whole-block update (its own kernel: its register-held
 // accumulators would lower the occupancy of the small-block update)
 template <typename T>
@@ -1611,19 +1530,6 @@ __global__ void __launch_bounds__(256) k_fwd(Problem<T> p, Level lv, const __gri
 // ---------------------------------------------------------------------------
 // k_bwd (level l, descending): x_i -= F_i^T x_{i+s} + G_i x_{i-s};  x_i <- C_i^{-T} x_i
 // ---------------------------------------------------------------------------
-// store_block, and with xacc also xacc[r * dst_ld + c] += dst value (in FP64)
-template <typename T>
-__device__ __forceinline__ void store_block_acc(T* dst, long long dst_ld, const T* src, int ld, int rows, int cols,
-                                                double* xacc) {
-  const int total = rows * cols;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int r = e / cols, c = e - r * cols;
-    const T v = src[r * ld + c];
-    dst[(long long)r * dst_ld + c] = v;
-    if (xacc != nullptr) xacc[(long long)r * dst_ld + c] += (double)v;
-  }
-}
-
 template <typename T, bool RES, bool INV>
 __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, int b, int t,
                                          unsigned char* smem_raw, const SweepMaps* tm = nullptr) {
@@ -1649,7 +1555,6 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
   const T* G = left ? p.Eb(b, slot - 1) : nullptr;
   const T* Li = p.Lb(b, i);
   T* xi = p.Xb(b, i);
-  double* xa = p.xacc == nullptr ? nullptr : p.xacc + (long long)b * p.sX + (long long)i * n * p.m;
   const ResTma tu = RES ? res_tma_begin(tm, smem_raw, bar) : ResTma{false, false};
   if (!lv.pre) pdl_wait();
   if (RES) {
@@ -1707,7 +1612,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
         else
           res_matvec<T, 2>(Z1, Y, ldy, mc, Cs, ldm, dv, n);
         __syncthreads();
-        store_block_acc(xi + c0, p.m, Z1, ldy, n, mc, xa == nullptr ? nullptr : xa + c0);
+        store_block(xi + c0, p.m, Z1, ldy, n, mc);
         continue;
       }
       res_tri_solve<T, true>(Y, ldy, mc, Cs, ldm, dv, n);
@@ -1715,7 +1620,7 @@ __device__ __forceinline__ void bwd_body(const Problem<T>& p, const Level& lv, i
       sweep_accumulate2<T, true, false>(Y, Z1, F, Z2, G, ldy, mc, n, Ms);
       sweep_upper_solve(Y, ldy, mc, Li, n, Ms, dv);
     }
-    store_block_acc(xi + c0, p.m, Y, ldy, n, mc, xa == nullptr ? nullptr : xa + c0);
+    store_block(xi + c0, p.m, Y, ldy, n, mc);
   }
 }
 

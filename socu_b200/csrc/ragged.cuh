@@ -250,7 +250,6 @@ __device__ __forceinline__ Problem<T> rg_problem(const RgArgs<T>& a, const RgIns
   p.X = a.X + I.oX;
   p.mask = nullptr;
   p.info = nullptr;
-  p.xacc = nullptr;
   p.B = 1;
   p.N = I.N;
   p.n = I.n;
@@ -284,6 +283,7 @@ __device__ __forceinline__ RefineArgs rg_refine_args(const RgArgs<T>& a, const R
   r.S = I.S;
   r.tol = a.tol;
   r.max_iter = a.max_iter;
+  r.check_in_residual = 0;
   return r;
 }
 

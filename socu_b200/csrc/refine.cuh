@@ -20,6 +20,8 @@ struct RefineState {
   unsigned long long bnorm; // ||b||_inf bits
   unsigned long long rnorm; // ||r||_inf bits, accumulated per iteration
   unsigned long long xnorm; // ||x||_inf bits, accumulated per iteration
+  unsigned done;            // residual CTAs of this round that have added their norms
+  unsigned pad;
 };
 
 struct RefineArgs {
@@ -40,6 +42,7 @@ struct RefineArgs {
   int B, N, n, m, S;
   double tol;
   int max_iter;
+  int check_in_residual;   // 1: the residual's last CTA per instance also runs the convergence test
 };
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
@@ -72,6 +75,7 @@ __global__ void k_ref_reset(RefineArgs a) {
     a.st[bi].bnorm = 0ull;
     a.st[bi].rnorm = 0ull;
     a.st[bi].xnorm = 0ull;
+    a.st[bi].done = 0u;
     if (on) atomicExch(a.any_active, 1);
   }
 }
@@ -150,6 +154,59 @@ __host__ __device__ inline long long smem_residual_elems(int n) {
 
 // REFINE: write R32 = float(r), accumulate norms, skip inactive instances.
 // Otherwise write r (double) to a.rout for every instance.
+// x += delta (R32) for active instances; grid-stride over the whole batch.
+__global__ void __launch_bounds__(256) k_ref_update(RefineArgs a) {
+  pdl_wait();
+  pdl_trigger();
+  const long long per = (long long)a.N * a.n * a.m;
+  const long long total = (long long)a.B * per;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int bi = (int)(e / per);
+    if (a.active[bi]) a.x[e] += (double)a.R32[e];
+  }
+}
+
+// Convergence test of instance bi; clears the accumulators for the next
+// round.  A non-finite eta (numerical breakdown of the float factor) stops the
+// instance with iters = -(iterations done).
+__device__ __forceinline__ void ref_check_instance(const RefineArgs& a, int bi) {
+  RefineState& s = a.st[bi];
+  // norms other CTAs added with atomics: read them the same way
+  const double rn = __longlong_as_double((long long)atomicAdd(&s.rnorm, 0ull));
+  const double xn = __longlong_as_double((long long)atomicAdd(&s.xnorm, 0ull));
+  const double pn = __longlong_as_double((long long)s.psi);
+  const double bn = __longlong_as_double((long long)s.bnorm);
+  const double den = pn * xn + bn;
+  const double eta = den > 0.0 ? rn / den : 0.0;
+  const int it = a.iters[bi] + 1;
+  a.iters[bi] = it;
+  a.eta[bi] = eta;
+  s.rnorm = 0ull;
+  s.xnorm = 0ull;
+  if (!(eta == eta) || isinf(eta)) {
+    a.active[bi] = 0;
+    a.iters[bi] = -it;
+  } else if (eta <= a.tol || it >= a.max_iter) {
+    a.active[bi] = 0;
+  } else {
+    atomicExch(a.any_active, 1);
+  }
+}
+
+// check_in_residual: thread 0 of every residual CTA of an active instance,
+// after its norms: the CTA that completes the instance's count runs the test
+// (and rearms the count), so no separate test launch follows the residual.
+__device__ __forceinline__ void residual_arrive(const RefineArgs& a, int bi, unsigned ctas) {
+  if (!a.check_in_residual || threadIdx.x != 0) return;
+  __threadfence();
+  if (atomicAdd(&a.st[bi].done, 1u) + 1u == ctas) {
+    __threadfence();
+    ref_check_instance(a, bi);
+    a.st[bi].done = 0u;
+  }
+}
+
 template <bool REFINE>
 __device__ __forceinline__ void residual_body(const RefineArgs& a, int bi, int i, int r0, unsigned char* smem_raw) {
   const int n = a.n, m = a.m, N = a.N;
@@ -227,6 +284,7 @@ __global__ void __launch_bounds__(256) k_residual(RefineArgs a) {
   if (REFINE && !a.active[bi]) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   residual_body<REFINE>(a, bi, i, (rem - i * nrc) * kResRows, smem_raw);
+  if (REFINE) residual_arrive(a, bi, (unsigned)per);
 }
 
 // ---------------------------------------------------------------------------
@@ -389,6 +447,7 @@ __global__ void __launch_bounds__(256, GR == 4 ? 2 : 3) k_residual_rows(RefineAr
   if (REFINE && !a.active[bi]) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   residual_rows_body<REFINE, GR>(a, bi, i, smem_raw);
+  if (REFINE) residual_arrive(a, bi, (unsigned)a.N);
 }
 
 // Refinement set-up for block row i (if i < N) and storage slot i (if i < S):
@@ -491,37 +550,6 @@ __global__ void __launch_bounds__(256) k_ref_init_rows(RefineArgs a) {
   if (a.mask != nullptr && a.mask[bi] == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ref_init_rows_body(a, bi, i, smem_raw);
-}
-
-// Convergence test per instance; clears the accumulators for the next round.
-// A non-finite eta (numerical breakdown of the float factor) stops the
-// instance with iters = -(iterations done).
-__global__ void k_ref_check(RefineArgs a) {
-  pdl_wait();
-  pdl_trigger();
-  for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < a.B; bi += gridDim.x * blockDim.x) {
-    if (!a.active[bi]) continue;
-    RefineState& s = a.st[bi];
-    const double rn = __longlong_as_double((long long)s.rnorm);
-    const double xn = __longlong_as_double((long long)s.xnorm);
-    const double pn = __longlong_as_double((long long)s.psi);
-    const double bn = __longlong_as_double((long long)s.bnorm);
-    const double den = pn * xn + bn;
-    const double eta = den > 0.0 ? rn / den : 0.0;
-    const int it = a.iters[bi] + 1;
-    a.iters[bi] = it;
-    a.eta[bi] = eta;
-    s.rnorm = 0ull;
-    s.xnorm = 0ull;
-    if (!(eta == eta) || isinf(eta)) {
-      a.active[bi] = 0;
-      a.iters[bi] = -it;
-    } else if (eta <= a.tol || it >= a.max_iter) {
-      a.active[bi] = 0;
-    } else {
-      atomicExch(a.any_active, 1);
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------

@@ -254,24 +254,3 @@ def test_register_chain_matches_shared_chain_bitwise(n):
         assert torch.equal(a, b)
     x_ref = nd.nd_factor_and_solve(L0, E0, b0)[2][0]
     assert np.abs(outs[0][2].double().cpu().numpy() - x_ref).max() <= 1e-4 * max(1.0, np.abs(x_ref).max())
-
-
-@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-@pytest.mark.parametrize("n", [16, 40, 64])
-def test_tile_updates_match_whole_block_updates_bitwise(dtype, n):
-    """On levels with at most one block per SM the n <= 64 Schur updates run as
-    one 32 x 32 tile per CTA; an explicit update_threads setting keeps the
-    whole-block update CTAs.  Same DMMA products in the same k order: the
-    factors must agree bit for bit."""
-    from socu_b200.block_tridiag_solver import _launch_with_settings
-
-    N, m = 100, 3
-    L0, E0, b0 = generators.readme_problem(N, n, m, shift=10.0 + 2.0 * np.sqrt(n), seed=11 + n)
-    outs = []
-    for settings in ({}, {"update_threads": 256}):
-        L, E, x = (torch.tensor(a, dtype=dtype, device=DEV) for a in (L0, E0, b0))
-        _launch_with_settings("factor_and_solve", L, E, x, dtype, settings)()
-        torch.cuda.synchronize()
-        outs.append((L, E, x))
-    for a, b in zip(outs[0], outs[1]):
-        assert torch.equal(a, b)
