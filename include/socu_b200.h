@@ -403,6 +403,18 @@ int socu_tc_selftest(const float* A, const float* B, float* D, int64_t m_rows, i
 int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,
                                 int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream);
 
+/* Copy the lower triangles of `count` consecutive row-major n x n blocks of
+ * elem_bytes-byte elements (the only part of L that every factor and the
+ * residual read) from src to dst, host or device memory on either side, in
+ * 16-row bands (band k: rows 16k.., columns 0 .. 16k+15) on `stream`: a
+ * caller streaming L from pinned host memory moves ~(n + 16) / 2n of the
+ * bytes.  Elements above the band diagonal of dst are left as they are.  No
+ * counterpart in the reference. */
+int socu_copy_lower_blocks_async(void* dst, const void* src, int64_t count, int64_t n, int64_t elem_bytes,
+                                 void* stream);
+/* Bytes socu_copy_lower_blocks_async moves for those arguments. */
+int64_t socu_lower_blocks_bytes(int64_t count, int64_t n, int64_t elem_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,8 @@ _SIGNATURES = {
                                                   _i64, _int, ctypes.c_double, _vp, ctypes.c_size_t, _vp, _vp, _vp,
                                                   _vp]),
     "socu_block_tridiag_residual": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
+    "socu_copy_lower_blocks_async": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
+    "socu_lower_blocks_bytes": (_i64, [_i64, _i64, _i64]),
     "socu_block_tridiag_grad": (_int, [_int, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
     "socu_refine_solve_noalloc": (_int, [_vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _int, ctypes.c_double,
                                          _vp, _vp, _vp]),

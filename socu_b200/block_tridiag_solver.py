@@ -371,3 +371,34 @@ def create_cholesky_solve_launch(L, E, x, mask=None, block_dim=None, block_size=
     op = _lib.OP_SOLVE_INV if factor_has_inverse else _lib.OP_SOLVE
     return _create(op, L, E, x, mask, dtype, device, stream, use_cuda_graph, True,
                    _settings(block_dim, block_size))
+
+
+# ---------------------------------------------------------------------------
+# extension: moving L to the device
+# ---------------------------------------------------------------------------
+
+def copy_lower_blocks(dst, src, stream=None):
+    """Copy the lower triangles of the n x n blocks of ``src`` into ``dst``
+    (same shape (..., n, n), contiguous, same dtype; pinned host or device
+    memory on either side), in 16-row bands, asynchronously on ``stream``
+    (default: the current stream of the device side).  Every factor and the
+    FP64 residual read only lower(L_i), so a caller that streams L from host
+    memory for each solve moves (n + 16) / 2n of its bytes (62.5 % at n = 64).
+    Elements of ``dst`` above the bands are left unchanged.  Returns the bytes
+    moved.  No counterpart in the reference."""
+    if dst.shape != src.shape or dst.dtype != src.dtype:
+        raise ValueError("dst and src must have the same shape and dtype")
+    if dst.dim() < 2 or dst.shape[-1] != dst.shape[-2]:
+        raise ValueError("blocks must be square: shape (..., n, n)")
+    if not (dst.is_contiguous() and src.is_contiguous()):
+        raise ValueError("dst and src must be contiguous")
+    n = int(dst.shape[-1])
+    count = dst.numel() // (n * n) if n else 0
+    dev = dst.device if dst.is_cuda else src.device
+    if dev.type != "cuda":
+        raise ValueError("one side must be CUDA memory")
+    sh = _stream_handle(stream if stream is not None else torch.cuda.current_stream(dev), dev)
+    lib = _lib.load()
+    _lib.check(lib.socu_copy_lower_blocks_async(ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(src.data_ptr()),
+                                                count, n, dst.element_size(), sh), "socu_copy_lower_blocks_async")
+    return int(lib.socu_lower_blocks_bytes(count, n, dst.element_size()))

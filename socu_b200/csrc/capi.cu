@@ -1650,6 +1650,39 @@ int socu_block_tridiag_grad(socu_dtype dtype, const void* x, const void* g, void
   return cuda_status(e != cudaSuccess ? e : cudaGetLastError());
 }
 
+constexpr int64_t kLowerBand = 16;
+
+int64_t socu_lower_blocks_bytes(int64_t count, int64_t n, int64_t elem_bytes) {
+  if (count < 0 || n <= 0 || elem_bytes <= 0) return 0;
+  int64_t per = 0;
+  for (int64_t r0 = 0; r0 < n; r0 += kLowerBand) {
+    const int64_t rows = std::min(kLowerBand, n - r0), cols = std::min(r0 + kLowerBand, n);
+    per += rows * cols;
+  }
+  return per * count * elem_bytes;
+}
+
+int socu_copy_lower_blocks_async(void* dst, const void* src, int64_t count, int64_t n, int64_t elem_bytes,
+                                 void* stream) {
+  if (dst == nullptr || src == nullptr || count < 0 || n <= 0 || elem_bytes <= 0) return SOCU_ERR_INVALID_ARGUMENT;
+  if (count == 0) return SOCU_OK;
+  const size_t pitch = (size_t)(n * elem_bytes);
+  for (int64_t r0 = 0; r0 < n; r0 += kLowerBand) {
+    const int64_t rows = std::min(kLowerBand, n - r0), cols = std::min(r0 + kLowerBand, n);
+    // one 3-D copy per band: width = the band's columns, height = its rows,
+    // depth = the blocks (slice pitch = one block)
+    cudaMemcpy3DParms prm = {};
+    const size_t off = (size_t)r0 * pitch;
+    prm.srcPtr = make_cudaPitchedPtr(const_cast<char*>(static_cast<const char*>(src)) + off, pitch, pitch, (size_t)n);
+    prm.dstPtr = make_cudaPitchedPtr(static_cast<char*>(dst) + off, pitch, pitch, (size_t)n);
+    prm.extent = make_cudaExtent((size_t)(cols * elem_bytes), (size_t)rows, (size_t)count);
+    prm.kind = cudaMemcpyDefault;
+    const cudaError_t e = cudaMemcpy3DAsync(&prm, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  return SOCU_OK;
+}
+
 int socu_block_tridiag_residual(const double* L, const double* E, const double* x, const double* b, double* r,
                                 int64_t batch, int64_t horizon, int64_t n, int64_t n_rhs, void* stream) {
   Dims d;
