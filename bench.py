@@ -52,10 +52,10 @@ TRAFFIC_NOTE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_bwd
 # DRAM bytes (read + write) per k_node<float, y, inverse> launch of a float
 # factor_and_solve of this shape, averaged over its 11 levels: ncu capture of
 # `bench.py --ncu-case node` (4 systems, so that the float blocks exceed L2),
-# 254.7 MB over the 11 launches of one pass, per system
+# 254.1 MB over the 11 launches of one pass, per system
 # (profiles/k_node_f32_levels_N1024_n64_m8_B4.md)
-NODE_TRAFFIC_BYTES = 254.66e6 / 4 / 11
-NODE_TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 11 k_node<float,1,1> launches of "
+NODE_TRAFFIC_BYTES = 254.13e6 / 4 / 11
+NODE_TRAFFIC_NOTE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 11 k_node<float,1,1,wt> launches of "
                      "bench.py --ncu-case node (4 systems, inputs > L2), per system and launch; "
                      "profiles/k_node_f32_levels_N1024_n64_m8_B4.md")
 RAGGED_WORKLOAD = ("4096 independent systems, N ~ U{8..256}, n in {8,16,32,48}, m in {1,4}, shift=10, "
