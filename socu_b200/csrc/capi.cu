@@ -17,6 +17,7 @@
 #include "ragged.cuh"
 #include "tc_node.cuh"
 #include "tc_update.cuh"
+#include "top_sweep.cuh"
 
 namespace socu {
 namespace {
@@ -310,6 +311,101 @@ void launch(void (*kernel)(KArgs...), unsigned blocks, unsigned threads, size_t 
   cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+// As launch(), as clusters of `cluster` CTAs along x (blocks a multiple of it).
+template <typename... KArgs, typename... Args>
+void launch_cluster(void (*kernel)(KArgs...), unsigned blocks, unsigned threads, size_t smem, cudaStream_t s,
+                    bool pdl, int cluster, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  int na = 1;
+  if (pdl && pdl_enabled()) {
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    na = 2;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// Clusters of `cluster` CTAs (threads, smem each) that fit the device at once,
+// cached per kernel, device and shape; 0 when the query fails (no device, or
+// the size is not supported).
+struct ClusterSlot {
+  const void* fn;
+  int dev, cluster, threads;
+  size_t smem;
+  int fits;
+};
+std::mutex g_cluster_mu;
+ClusterSlot g_cluster[kCacheSlots];
+int g_n_cluster = 0;
+
+template <typename K>
+int cluster_capacity(K kernel, int cluster, int threads, size_t smem) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  const void* fn = reinterpret_cast<const void*>(kernel);
+  {
+    std::lock_guard<std::mutex> g(g_cluster_mu);
+    for (int i = 0; i < g_n_cluster; ++i)
+      if (g_cluster[i].fn == fn && g_cluster[i].dev == dev && g_cluster[i].cluster == cluster &&
+          g_cluster[i].threads == threads && g_cluster[i].smem == smem)
+        return g_cluster[i].fits;
+  }
+  int fits = 0;
+  cudaError_t e = prepare(kernel, smem);
+  if (e == cudaSuccess && cluster > 8) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cluster);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaOccupancyMaxActiveClusters(&fits, kernel, &cfg);
+  }
+  if (e != cudaSuccess) {
+    fits = 0;
+    (void)cudaGetLastError();   // a refused size only means "no cluster kernel"
+  }
+  std::lock_guard<std::mutex> g(g_cluster_mu);
+  if (g_n_cluster < kCacheSlots) g_cluster[g_n_cluster++] = ClusterSlot{fn, dev, cluster, threads, smem, fits};
+  return fits;
+}
+
+// SOCU_TOP_SWEEP=1 runs the top levels of the sweeps in the cluster-resident
+// k_top instead of one launch per level.  Off by default: measured on B200,
+// the per-level launches of a graph (programmatic dependent launch, blocks
+// loaded before the dependency wait) are faster at every shape tried -- a
+// float solve on an inverse-carrying factor at N=1024, n=64, m=8 takes 132 us
+// with a launch per level vs 153 us with k_top, at N=20, n=16, m=1 29 vs 35 us
+// (one k_top launch instead of ten): the cluster barrier and the L2 reads of
+// the vectors after it cost more per level than a kernel boundary.
+bool top_sweep_enabled() {
+  static const int on = [] {
+    const char* v = std::getenv("SOCU_TOP_SWEEP");
+    return (v != nullptr && v[0] == '1') ? 1 : 0;
+  }();
+  return on != 0;
+}
+
 // ---------------------------------------------------------------------------
 // TMA tensor maps of the resident sweeps.  cuTensorMapEncodeTiled is a
 // driver-API call; it is resolved through the runtime's entry-point query, so
@@ -591,6 +687,65 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
   };
   const bool forked = run && fork != nullptr && fork->ok();
 
+  // On request (SOCU_TOP_SWEEP=1), the top levels of the sweeps in one
+  // cluster-resident kernel (k_top): the forward levels with at most `cluster`
+  // tasks and the backward levels with at most `cluster` nodes, one cluster per
+  // instance, when every instance's cluster fits the device at once (otherwise
+  // the per-level launches parallelise better).  The decision needs the device;
+  // without one (counting on a host without a GPU) every level keeps its own
+  // launch.
+  const bool want_fwd = op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE;
+  const bool want_bwd =
+      op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE;
+  auto top_kernel = inv ? k_top<T, true> : k_top<T, false>;
+  TopLevels top;
+  std::memset(&top, 0, sizeof top);
+  int top_cluster = 0;
+  size_t top_smem = 0;
+  const int top_thr = swp_thr;
+  if (res && p.m > 0 && top_sweep_enabled() && (want_fwd || want_bwd)) {
+    for (int stages = 2; stages >= 1 && top_smem == 0; --stages) {
+      const size_t bytes = (size_t)smem_top_elems(n, p.m, stages) * sizeof(T);
+      if (bytes <= (size_t)max_smem_optin()) {
+        top_smem = bytes;
+        top.stages = stages;
+      }
+    }
+    for (int cl = 16; top_smem > 0 && cl >= 4 && top_cluster == 0; cl /= 2) {
+      int flo = K, blo = K;
+      if (want_fwd)
+        while (flo > 0 && K - flo < kTopMaxLevels && fwd_tasks(p.N, lv[flo - 1]) <= cl) --flo;
+      if (want_bwd)
+        while (blo > 0 && K - blo < kTopMaxLevels && lv[blo - 1].d <= cl) --blo;
+      if ((K - flo) + (K - blo) < 2) break;
+      int widest = 1;
+      for (int l = flo; l < K; ++l) widest = std::max(widest, fwd_tasks(p.N, lv[l]));
+      for (int l = blo; l < K; ++l) widest = std::max(widest, lv[l].d);
+      int c = 1;
+      while (c < widest) c *= 2;
+      if (cluster_capacity(top_kernel, c, top_thr, top_smem) < p.B) continue;
+      top_cluster = c;
+      top.fwd_lo = flo;
+      top.fwd_n = K - flo;
+      top.bwd_lo = blo;
+      top.bwd_n = K - blo;
+      top.pre = op != SOCU_OP_FACTOR_AND_SOLVE ? 1 : 0;
+      for (int l = flo; l < K; ++l)
+        top.fl[l - flo] = sweep_level(lv[l], (long long)p.B * fwd_tasks(p.N, lv[l]), true);
+      for (int l = blo; l < K; ++l) top.bl[l - blo] = sweep_level(lv[l], (long long)p.B * lv[l].d, true);
+    }
+  }
+  auto go_top = [&]() {
+    ++launches;
+    if (!run) return;
+    const bool pdl = !first && g_prof == nullptr;
+    first = false;
+    prof_begin(st, top.bwd_n > 0 ? SOCU_KIND_BACKWARD : SOCU_KIND_FORWARD);
+    launch_cluster(top_kernel, (unsigned)((long long)p.B * top_cluster), (unsigned)top_thr, top_smem, st, pdl,
+                   top_cluster, p, top, maps);
+    prof_end(st);
+  };
+
   const bool factor = op == SOCU_OP_FACTOR || op == SOCU_OP_FACTOR_AND_SOLVE;
   if (factor && p.info != nullptr) {
     ++launches;
@@ -667,13 +822,14 @@ int enqueue(socu_op op, const Problem<T>& p, cudaStream_t st, long long* count, 
     }
   }
   if (op == SOCU_OP_FORWARD_SUBSTITUTION || op == SOCU_OP_SOLVE) {
-    for (int l = 0; l < K; ++l) {
+    for (int l = 0; l < (top_cluster ? top.fwd_lo : K); ++l) {
       const long long blocks = (long long)p.B * (l == 0 ? lv[l].d : p.N / lv[l].s);
       go_on(st, fwd_kernel, SOCU_KIND_FORWARD, blocks, ss, sweep_level(lv[l], blocks, true), swp_thr, maps);
     }
   }
+  if (top_cluster) go_top();
   if (op == SOCU_OP_BACKWARD_SUBSTITUTION || op == SOCU_OP_SOLVE || op == SOCU_OP_FACTOR_AND_SOLVE) {
-    for (int l = K - 1; l >= 0; --l) {
+    for (int l = (top_cluster ? top.bwd_lo : K) - 1; l >= 0; --l) {
       const long long blocks = (long long)p.B * lv[l].d;
       go_on(st, bwd_kernel, SOCU_KIND_BACKWARD, blocks, ss,
             sweep_level(lv[l], blocks, op != SOCU_OP_FACTOR_AND_SOLVE || l != K - 1), swp_thr, maps);
