@@ -540,8 +540,12 @@ def run_ours(args, rank, world, local_rank):
         "phases": dict(budget(phases_mixed), note="one eager run with CUDA events around every kernel, "
                        f"{abs(iters)} rounds; events add gaps, so the sum exceeds ms_per_step"),
         "roofline": {"kernel": f"k_node<float> (level nodes of the mixed solve: potrf + coupling solves + forward "
-                               f"step, averaged over its launches; phase with the largest share of this run's "
-                               f"eager profile: {dom})",
+                               f"step, averaged over its launches; the kernel with the most device time in the "
+                               f"mixed solve's ncu launch list; this run's eager profile: node "
+                               f"{node_ms:.3f} ms in {node_launches} launches, backward sweeps "
+                               f"{phases_mixed.get('backward', (0.0, 0))[0]:.3f} ms in "
+                               f"{phases_mixed.get('backward', (0.0, 0))[1]}, "
+                               f"largest phase {dom})",
                      "bound": "tensor", "achieved": node_ach, "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": node_ach / bf16_peak, "peak_source": f"{peak_src} (bf16 dense, MEASURED_PEAKS.json)",
                      "traffic": NODE_TRAFFIC_BYTES, "traffic_source": NODE_TRAFFIC_NOTE,
