@@ -772,7 +772,8 @@ def run_ncu_case(name):
     L, E, b = readme_blocks(c["N"], c["n"], c["m"], shift=c["shift"], seed=SEED, batch=c["B"], device="cuda")
     for dt in (torch.float32, torch.float64):
         for _ in range(2):
-            Lw, Ew, xw = L.to(dt), E.to(dt), b.to(dt)
+            # copies: the FP64 inputs must stay intact for the next pass and the mixed solve
+            Lw, Ew, xw = L.to(dt, copy=True), E.to(dt, copy=True), b.to(dt, copy=True)
             create_cholesky_factor_and_solve_launch(Lw, Ew, xw, dtype=dt)()
             torch.cuda.synchronize()
     if c["n"] > 64:
